@@ -1,0 +1,100 @@
+/*
+ * pfsf_b200.h -- additive exports of the B200 build (ABI MINOR additions:
+ * no existing struct, enum value or signature changes).
+ *
+ * The reference tick runs a fixed 16-step schedule and never iterates to a
+ * tolerance.  These entry points add a solve of the symmetric per-link
+ * 26-point operator
+ *     sum_j w_ij (phi_i - phi_j) = s_i     (solid voxels i)
+ *     w_ij = {1, 0.5, 1/6}[face/edge/corner] * 2 k_i k_j / (k_i + k_j)
+ * (anchors Dirichlet phi = 0, air and out-of-box links dropped) to a relative
+ * residual ||s - A phi||_2 / ||s||_2 <= rel_tol, for all listed islands,
+ * either island by island (plain FP32) or batched in one persistent launch
+ * with reduced-precision coefficient storage and FP32 residual refinement.
+ */
+#ifndef PFSF_B200_H
+#define PFSF_B200_H
+#include "pfsf_types.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PFSF_PREC_FP32 = 0, /* kappa and coarse levels stored FP32 */
+    PFSF_PREC_BF16 = 1, /* kappa and coarse levels stored BF16 */
+    PFSF_PREC_FP16 = 2, /* kappa and coarse levels stored FP16 */
+} pfsf_precision;
+
+typedef enum {
+    PFSF_SOLVE_PER_ISLAND = 0, /* one island at a time, one kernel per step */
+    PFSF_SOLVE_BATCHED = 1,    /* all islands in one persistent launch */
+} pfsf_solve_mode;
+
+/* flags of pfsf_solve_to_tolerance */
+#define PFSF_SOLVE_NO_UPLOAD 0x1u   /* inputs already resident on the device */
+#define PFSF_SOLVE_NO_READBACK 0x2u /* leave phi on the device */
+
+/* Caller-owned host arrays of one island for the tolerance solve. */
+typedef struct pfsf_island_kappa_buffers {
+    void* phi_addr; /* float32 x N: initial guess in, solution out */
+    int64_t phi_bytes;
+    void* source_addr; /* float32 x N */
+    int64_t source_bytes;
+    void* kappa_addr; /* float32 x N, per-voxel conductivity (> 0 on non-air) */
+    int64_t kappa_bytes;
+    void* voxel_type_addr; /* uint8 x N */
+    int64_t voxel_type_bytes;
+} pfsf_island_kappa_buffers;
+
+typedef struct pfsf_solve_stats {
+    int32_t struct_bytes;
+    int32_t islands_solved;
+    int32_t islands_converged;
+    int32_t max_iterations;  /* largest outer iteration count over islands */
+    double max_rel_residual; /* largest final ||s - A phi|| / ||s|| (FP64) */
+    float device_ms;         /* solve time on the engine stream (CUDA events) */
+    float upload_ms;
+    float readback_ms;
+    int32_t kernel_launches; /* kernels launched by the solve */
+} pfsf_solve_stats;
+
+/* Registers the kappa-form inputs of an island created by pfsf_add_island.
+ * NULL pointers or undersized arrays -> PFSF_ERROR_INVALID_ARG. */
+PFSF_API pfsf_result pfsf_register_island_kappa(pfsf_engine engine, int32_t island_id,
+                                                const pfsf_island_kappa_buffers* bufs);
+PFSF_API void pfsf_set_precision_mode(pfsf_engine engine, pfsf_precision mode);
+PFSF_API void pfsf_set_solve_mode(pfsf_engine engine, pfsf_solve_mode mode);
+
+/* Solves every listed island to rel_tol (max_iter outer iterations at most)
+ * and writes phi back to its registered phi array.  Returns PFSF_OK even if
+ * some island did not converge (see out->islands_converged). */
+PFSF_API pfsf_result pfsf_solve_to_tolerance(pfsf_engine engine, const int32_t* island_ids, int32_t count,
+                                             double rel_tol, int32_t max_iter, uint32_t flags,
+                                             pfsf_solve_stats* out);
+
+/* Copies the FP64 solution accumulator of the last tolerance solve of an
+ * island (count = min(N, capacity) values).  The FP32 phi written back by
+ * pfsf_solve_to_tolerance is this vector rounded to float32. */
+PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine engine, int32_t island_id, double* out, int64_t capacity,
+                                          int64_t* out_count);
+
+/* Diagnostic read of the per-island tick state (not part of the reference
+ * ABI; used by parity tests and tooling).  field: 0 phi (float32 x N),
+ * 1 history H (float32 x N), 2 damage d (float32 x N), 3 failure flags
+ * (uint8 x N), 4 macro-block residual bits (uint32 x blocks), 5 schedule state
+ * {int32 chebyshev_iter, pcg_allocated, mg_allocated, float prev, last macro
+ * residual} (20 bytes).  Copies min(bytes, field size); *out_bytes gets the
+ * field size. */
+PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine engine, int32_t island_id, int32_t field, void* out,
+                                           int64_t bytes, int64_t* out_bytes);
+
+/* The cudaStream_t the engine launches on (for event timing by callers). */
+PFSF_API void* pfsf_get_stream(pfsf_engine engine);
+
+/* Number of kernels this engine has launched since creation. */
+PFSF_API int64_t pfsf_kernel_launch_count(pfsf_engine engine);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,241 @@
+"""ctypes front-end of the CPU oracle (``liboracle.so`` built from pfsf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py``.  The product library never imports it.
+
+Each wrapper names the reference shader or host routine it restates (paths
+relative to the PFSF-CORE checkout, SH = .../shaders/compute/pfsf).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+U8P = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+U32P = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (gcc, FP contraction off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "pfsf_oracle.c")
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        i = C.c_int
+        L.o_rbgs_color.argtypes = [i, i, i, F32P, F32P, F32P, U8P, F32P, U32P, i, C.c_float]
+        L.o_rbgs_step.argtypes = [i, i, i, F32P, F32P, F32P, U8P, F32P, U32P, C.c_float]
+        L.o_jacobi_coarse.argtypes = [i, i, i, F32P, F32P, F32P, F32P, U8P, F32P, C.c_float]
+        L.o_restrict.argtypes = [i, i, i, F32P, F32P, F32P, U8P, i, i, i, F32P, F32P]
+        L.o_prolong.argtypes = [i, i, i, F32P, i, i, i, F32P]
+        L.o_downsample.argtypes = [i, i, i, F32P, U8P, i, i, i, F32P, U8P]
+        L.o_pcg_precompute.argtypes = [i, i, i, F32P, F32P]
+        L.o_pcg_matvec.argtypes = [i, i, i, F32P, F32P, F32P, U8P]
+        L.o_pcg_update.argtypes = [i, i, i, F32P, F32P, F32P, F32P, F32P, F32P, U8P, F32P, F32P, F32P, i]
+        L.o_pcg_update.restype = C.c_double
+        L.o_pcg_direction.argtypes = [i, i, i, F32P, F32P, U8P, F32P, F32P]
+        L.o_rtz_limit.argtypes = [C.c_int64]
+        L.o_rtz_limit.restype = C.c_int64
+        L.o_phase_field.argtypes = [i, i, i, F32P, F32P, F32P, F32P, U8P, U32P, F32P, C.c_float, C.c_float,
+                                    C.c_float, i]
+        L.o_failure_scan.argtypes = [i, i, i, F32P, F32P, F32P, F32P, U8P, U32P, F32P, U32P, F32P, C.c_float]
+        L.pfo_create.argtypes = [i, i, i]
+        L.pfo_create.restype = C.c_void_p
+        L.pfo_destroy.argtypes = [C.c_void_p]
+        L.pfo_ptr.argtypes = [C.c_void_p, i]
+        L.pfo_ptr.restype = C.c_void_p
+        L.pfo_get_state.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
+        L.pfo_set_flags.argtypes = [C.c_void_p, i, i]
+        L.o_tick.argtypes = [C.c_void_p]
+        L.o_solve_steps.argtypes = [C.c_void_p, i]
+        L.o_solve_steps.restype = i
+        L.o_readback_failures.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]
+        L.o_readback_failures.restype = C.c_int32
+        L.o_kappa_apply.argtypes = [i, i, i, F64P, U8P, F64P, F64P]
+        L.o_kappa_pcg64.argtypes = [i, i, i, F64P, U8P, F64P, F64P, C.c_double, i, C.POINTER(C.c_double)]
+        L.o_kappa_pcg64.restype = i
+        L.o_kappa_relres.argtypes = [i, i, i, F64P, U8P, F64P, F32P]
+        L.o_kappa_relres.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# ---------------------------------------------------------------- kernels
+def rbgs_color(dims, phi, rho, sigma, vtype, H, macro, color, damping):
+    """SH/rbgs_smooth.comp.glsl:73-211 (one colour pass, in place on phi/H)."""
+    lx, ly, lz = dims
+    lib().o_rbgs_color(lx, ly, lz, phi, _c(rho, np.float32), _c(sigma, np.float32), _c(vtype, np.uint8), H,
+                       _c(macro, np.uint32), int(color), float(damping))
+
+
+def rbgs_step(dims, phi, rho, sigma, vtype, H, macro, damping):
+    lx, ly, lz = dims
+    lib().o_rbgs_step(lx, ly, lz, phi, _c(rho, np.float32), _c(sigma, np.float32), _c(vtype, np.uint8), H,
+                      _c(macro, np.uint32), float(damping))
+
+
+def jacobi_coarse(dims, phi, phi_prev, rho, sigma, vtype, Hfine, damping):
+    """SH/jacobi_smooth.comp.glsl:60-227 with omega=1, reading a pre-pass snapshot."""
+    lx, ly, lz = dims
+    lib().o_jacobi_coarse(lx, ly, lz, phi, _c(phi_prev, np.float32), _c(rho, np.float32),
+                          _c(sigma, np.float32), _c(vtype, np.uint8), Hfine, float(damping))
+
+
+def restrict(fdims, phi_f, rho_f, sig_f, type_f, cdims, phi_c, rho_c):
+    """SH/mg_restrict.comp.glsl:118-195."""
+    lib().o_restrict(*fdims, _c(phi_f, np.float32), _c(rho_f, np.float32), _c(sig_f, np.float32),
+                     _c(type_f, np.uint8), *cdims, phi_c, rho_c)
+
+
+def prolong(fdims, phi_f, cdims, phi_c):
+    """SH/mg_prolong.comp.glsl:233-275 (adds into phi_f)."""
+    lib().o_prolong(*fdims, phi_f, *cdims, _c(phi_c, np.float32))
+
+
+def downsample(sdims, cond, vtype, ddims):
+    """L1-native/libpfsf/src/core/island_buffer.cpp:600-700 (downsampleLevel)."""
+    dn = int(np.prod(ddims))
+    oc = np.zeros(6 * dn, np.float32)
+    ot = np.zeros(dn, np.uint8)
+    lib().o_downsample(*sdims, _c(cond, np.float32), _c(vtype, np.uint8), *ddims, oc, ot)
+    return oc, ot
+
+
+def pcg_precompute(dims, sigma):
+    n = int(np.prod(dims))
+    out = np.zeros(n, np.float32)
+    lib().o_pcg_precompute(*dims, _c(sigma, np.float32), out)
+    return out
+
+
+def pcg_matvec(dims, x, sigma, vtype):
+    n = int(np.prod(dims))
+    out = np.zeros(n, np.float32)
+    lib().o_pcg_matvec(*dims, _c(x, np.float32), out, _c(sigma, np.float32), _c(vtype, np.uint8))
+    return out
+
+
+def pcg_update(dims, phi, r, r_prev, p, ap, src, vtype, sigma, invdiag, red, is_init):
+    return lib().o_pcg_update(*dims, phi, r, _c(r_prev, np.float32), p, _c(ap, np.float32), _c(src, np.float32),
+                              _c(vtype, np.uint8), _c(sigma, np.float32), _c(invdiag, np.float32),
+                              _c(red, np.float32), int(is_init))
+
+
+def pcg_direction(dims, r, p, vtype, red, sigma):
+    lib().o_pcg_direction(*dims, _c(r, np.float32), p, _c(vtype, np.uint8), _c(red, np.float32),
+                          _c(sigma, np.float32))
+
+
+def rtz_limit(n):
+    return int(lib().o_rtz_limit(int(n)))
+
+
+def phase_field(dims, phi, H, D, sigma, vtype, fail, hyd, l0=2.0, gc=100.0, relax=0.3, split=1):
+    lib().o_phase_field(*dims, _c(phi, np.float32), _c(H, np.float32), D, _c(sigma, np.float32),
+                        _c(vtype, np.uint8), fail, _c(hyd, np.float32), l0, gc, relax, split)
+
+
+def failure_scan(dims, phi, sigma, maxphi, rcomp, vtype, fail, rtens, macro, rho, phi_orphan=1e6):
+    lib().o_failure_scan(*dims, _c(phi, np.float32), _c(sigma, np.float32), _c(maxphi, np.float32),
+                         _c(rcomp, np.float32), _c(vtype, np.uint8), fail, _c(rtens, np.float32), macro,
+                         _c(rho, np.float32), phi_orphan)
+
+
+# ---------------------------------------------------------------- island state
+class Island:
+    """One island with the native engine's per-island device state
+    (L1-native/libpfsf/src/core/island_buffer.h), held on the host."""
+
+    FIELDS = {"phi": (0, np.float32, 1), "source": (1, np.float32, 1), "conductivity": (2, np.float32, 6),
+              "type": (3, np.uint8, 1), "rcomp": (4, np.float32, 1), "rtens": (5, np.float32, 1),
+              "max_phi": (6, np.float32, 1), "hydration": (7, np.float32, 1), "H": (8, np.float32, 1),
+              "D": (9, np.float32, 1), "fail": (10, np.uint32, 1)}
+
+    def __init__(self, lx, ly, lz, pcg_enabled=True, phase_field=True):
+        self.dims = (int(lx), int(ly), int(lz))
+        self.n = lx * ly * lz
+        self._h = lib().pfo_create(lx, ly, lz)
+        lib().pfo_set_flags(self._h, int(pcg_enabled), int(phase_field))
+        self.nmb = ((lx + 7) // 8) * ((ly + 7) // 8) * ((lz + 7) // 8)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().pfo_destroy(self._h)
+            self._h = None
+
+    def view(self, name):
+        idx, dt, mult = self.FIELDS[name]
+        ptr = lib().pfo_ptr(self._h, idx)
+        n = self.n * mult
+        buf = (C.c_byte * (n * np.dtype(dt).itemsize)).from_address(ptr)
+        return np.frombuffer(buf, dtype=dt, count=n)
+
+    def macro(self):
+        ptr = lib().pfo_ptr(self._h, 11)
+        buf = (C.c_byte * (self.nmb * 4)).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.uint32, count=self.nmb)
+
+    def load(self, **arrays):
+        for k, v in arrays.items():
+            self.view(k)[:] = np.asarray(v).reshape(-1)
+
+    def state(self):
+        iv = (C.c_int32 * 3)()
+        fv = (C.c_float * 2)()
+        lib().pfo_get_state(self._h, iv, fv)
+        return {"chebyshev_iter": iv[0], "pcg_allocated": iv[1], "mg_allocated": iv[2],
+                "prev_macro": fv[0], "last_macro": fv[1]}
+
+    def tick(self):
+        """One dirty-island tick (L1-native/libpfsf/src/pfsf_engine.cpp:470-513)."""
+        lib().o_tick(self._h)
+
+    def failures(self, origin, capacity=1024, dbb=None):
+        """Failure DBB {count}{x,y,z,type}*k (island_buffer.cpp:864-966)."""
+        if dbb is None:
+            dbb = np.zeros(1 + 4 * capacity, np.int32)
+        lib().o_readback_failures(self._h, int(origin[0]), int(origin[1]), int(origin[2]),
+                                  dbb.ctypes.data, dbb.nbytes)
+        return dbb
+
+
+# ---------------------------------------------------------------- kappa operator
+def kappa_apply(dims, kappa, vtype, x):
+    n = int(np.prod(dims))
+    y = np.zeros(n, np.float64)
+    lib().o_kappa_apply(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(x, np.float64), y)
+    return y
+
+
+def kappa_solve64(dims, kappa, vtype, source, tol=1e-12, maxit=20000, x0=None):
+    """FP64 Jacobi-PCG on the symmetric harmonic-mean 26-point operator."""
+    n = int(np.prod(dims))
+    x = np.zeros(n, np.float64) if x0 is None else np.array(x0, np.float64)
+    rr = C.c_double(0.0)
+    it = lib().o_kappa_pcg64(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(source, np.float64), x,
+                             float(tol), int(maxit), C.byref(rr))
+    return x, it, rr.value
+
+
+def kappa_relres(dims, kappa, vtype, source, phi32):
+    return lib().o_kappa_relres(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(source, np.float64),
+                                _c(phi32, np.float32))

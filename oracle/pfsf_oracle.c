@@ -1,0 +1,998 @@
+/*
+ * pfsf_oracle.c -- CPU restatement of PFSF-CORE's per-tick structural solve.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.  The
+ * product library (pfsf-core_b200/) never links, calls or falls back to it.
+ *
+ * What it restates (reference paths relative to the PFSF-CORE checkout;
+ * SH = Block Reality/api/src/main/resources/assets/blockreality/shaders/compute/pfsf,
+ * NP = L1-native/libpfsf):
+ *   o_rbgs_color        SH/rbgs_smooth.comp.glsl:73-211
+ *   o_jacobi_coarse     SH/jacobi_smooth.comp.glsl:60-227
+ *   o_restrict          SH/mg_restrict.comp.glsl:39-195
+ *   o_prolong           SH/mg_prolong.comp.glsl:233-275
+ *   o_downsample        NP/src/core/island_buffer.cpp:600-700 (uploadMultigridData)
+ *   o_pcg_precompute    SH/pcg_precompute.comp.glsl:24-86
+ *   o_pcg_matvec        SH/pcg_matvec.comp.glsl:128-214
+ *   o_pcg_update        SH/pcg_update.comp.glsl:116-211
+ *   o_pcg_direction     SH/pcg_direction.comp.glsl:336-379
+ *   o_pcg_dot           SH/pcg_dot.comp.glsl (pass 1 + pass 2)
+ *   o_phase_field       SH/phase_field_evolve.comp.glsl:246-364
+ *   o_failure_scan      SH/failure_scan.comp.glsl:36-196
+ *   o_tick              NP/src/pfsf_engine.cpp:424-600 with the schedule of
+ *                       NP/src/solver/dispatcher.cpp:106-238,
+ *                       dispatcher_vcycle.cpp:315-392, dispatcher_pcg.cpp:254-298
+ *   o_kappa_*           symmetric per-link 26-point operator (harmonic-mean
+ *                       link conductivity) and an FP64 Jacobi-PCG that solves it
+ *                       to a tight tolerance ("exact" reference solution).
+ *
+ * Arithmetic is FP32 in the order the shaders write it; the FP64 solve is
+ * separate.  Where the reference is non-deterministic or reads out of
+ * bounds, the restatement fixes one deterministic reading (documented at
+ * each site and in DESIGN.md):
+ *   - jacobi_smooth binds phiPrev == phi (in-place, racy): restated as a
+ *     Jacobi pass that reads a snapshot taken before the pass.
+ *   - pcg_update reads neighbour r[j] while other workgroups rewrite it:
+ *     restated as reading r as it was before the dispatch.
+ *   - coarse type buffers are uint8 but the shaders declare uint32: restated
+ *     as one type per coarse cell (the data the host uploads).
+ *
+ * Parity status: the reference publishes no solver outputs (its fixtures
+ * hold inputs only), and its arithmetic runs only as Vulkan GLSL, which
+ * cannot be run here.  This restatement is pinned by the reference's own
+ * known-answer invariants (tests/test_oracle_pins.py): source-free island
+ * gives phi == 0, an isolated voxel gives phi == 0 and NO_SUPPORT, the
+ * analytic cantilever, stencil constants, and the 8-colour independence.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define EDGE_P 0.5f
+#define CORNER_P 0.1666667f
+#define MACRO_BLOCK 8
+#define MACRO_SEED_BITS 0x38D1B717u /* 1e-4f, island_buffer.cpp recordClearMacroResiduals */
+#define WARMUP_STEPS 8
+#define DAMPING_FACTOR 0.995f
+#define MG_INTERVAL 4
+#define STEPS_MAJOR 16
+#define PCG_MIN_RBGS 2
+#define PCG_MIN_STEPS 1
+#define PCG_MAX_N (512LL * 512LL)
+#define PHI_ORPHAN 1e6f
+#define PF_L0 2.0f /* max(PHASE_FIELD_L0=1.5, 2), dispatcher.cpp:244 */
+#define PF_GC 100.0f
+#define PF_RELAX 0.3f
+
+static inline int64_t gidx(int x, int y, int z, int lx, int ly) {
+    return (int64_t)x + (int64_t)lx * ((int64_t)y + (int64_t)ly * z);
+}
+static inline int finitef_(float v) { return !isnan(v) && !isinf(v); }
+static inline float clampf_(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+
+/* 26-point one-sided weights of voxel i, built from its own 6 face sigmas.
+ * Order: 6 faces (d=0..5), 12 edges (XY: --,++,-+,+-; XZ: same; YZ: same),
+ * 8 corners (ci bit0=x, bit1=y, bit2=z; bit set = +1).  Offsets in OFS. */
+static const int OFS[26][3] = {
+    {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1},
+    {-1, -1, 0}, {1, 1, 0}, {-1, 1, 0}, {1, -1, 0},
+    {-1, 0, -1}, {1, 0, 1}, {-1, 0, 1}, {1, 0, -1},
+    {0, -1, -1}, {0, 1, 1}, {0, -1, 1}, {0, 1, -1},
+    {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
+    {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+/* face-direction pair of each edge (a, b) */
+static const int EDGE_DIRS[12][2] = {{0, 2}, {1, 3}, {0, 3}, {1, 2}, {0, 4}, {1, 5},
+                                     {0, 5}, {1, 4}, {2, 4}, {3, 5}, {2, 5}, {3, 4}};
+
+static inline float edge_w(const float s6[6], int e) {
+    return sqrtf(fmaxf(s6[EDGE_DIRS[e][0]] * s6[EDGE_DIRS[e][1]], 0.0f)) * EDGE_P;
+}
+static inline float corner_w(const float s6[6], int ci) {
+    float sxc = (ci & 1) ? s6[1] : s6[0];
+    float syc = (ci & 2) ? s6[3] : s6[2];
+    float szc = (ci & 4) ? s6[5] : s6[4];
+    return cbrtf(fmaxf(sxc * syc * szc, 0.0f)) * CORNER_P;
+}
+static inline int inb(int x, int y, int z, int lx, int ly, int lz) {
+    return x >= 0 && x < lx && y >= 0 && y < ly && z >= 0 && z < lz;
+}
+static inline float safe_at(const float *a, int x, int y, int z, int lx, int ly, int lz) {
+    return inb(x, y, z, lx, ly, lz) ? a[gidx(x, y, z, lx, ly)] : 0.0f;
+}
+
+/* ---- shared stencil accumulation (rbgs_smooth.comp.glsl:125-176, also
+ *      jacobi_smooth.comp.glsl:123-180 with a different phi source) ---- */
+static void gs_accum(const float *phi_nb, const float *sigma, int64_t N, int64_t i,
+                     int x, int y, int z, int lx, int ly, int lz,
+                     float *sumSigma, float *sumNeighbor, float nphi6[6]) {
+    float s6[6];
+    int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+    float ss = 0.0f, sn = 0.0f;
+    for (int d = 0; d < 6; d++) {
+        s6[d] = sigma[(int64_t)d * N + i];
+        nphi6[d] = safe_at(phi_nb, x + OFS[d][0], y + OFS[d][1], z + OFS[d][2], lx, ly, lz);
+    }
+    for (int d = 0; d < 6; d++) {
+        if (!valid[d]) continue;
+        float s = s6[d];
+        if (s > 0.0f) {
+            float np = nphi6[d];
+            if (finitef_(np)) { ss += s; sn += s * np; }
+        }
+    }
+    for (int e = 0; e < 12; e++) {
+        if (!(valid[EDGE_DIRS[e][0]] && valid[EDGE_DIRS[e][1]])) continue;
+        float es = edge_w(s6, e);
+        if (es > 0.0f) {
+            const int *o = OFS[6 + e];
+            float ep = safe_at(phi_nb, x + o[0], y + o[1], z + o[2], lx, ly, lz);
+            if (finitef_(ep)) { ss += es; sn += es * ep; }
+        }
+    }
+    for (int ci = 0; ci < 8; ci++) {
+        const int *o = OFS[18 + ci];
+        if (!inb(x + o[0], y + o[1], z + o[2], lx, ly, lz)) continue;
+        float cs = corner_w(s6, ci);
+        if (cs > 0.0f) {
+            float cp = phi_nb[gidx(x + o[0], y + o[1], z + o[2], lx, ly)];
+            if (finitef_(cp)) { ss += cs; sn += cs * cp; }
+        }
+    }
+    *sumSigma = ss;
+    *sumNeighbor = sn;
+}
+
+static float amor_psi(const float *sigma, int64_t N, int64_t i, const float nphi6[6],
+                      int x, int y, int z, int lx, int ly, int lz, float phi_new) {
+    int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+    float fin = 0.0f, fout = 0.0f;
+    for (int d = 0; d < 6; d++) {
+        if (!valid[d]) continue;
+        float s = sigma[(int64_t)d * N + i];
+        if (s <= 0.0f) continue;
+        float flow = s * (nphi6[d] - phi_new);
+        if (flow > 0.0f) fin += flow;
+        else fout -= flow;
+    }
+    float k_comp = (fin > 3.0f * fout) ? 0.01f : 1.0f;
+    return 0.5f * phi_new * phi_new * k_comp;
+}
+
+/* ---- rbgs_smooth.comp.glsl:73-211, one colour pass, in place ---- */
+void o_rbgs_color(int lx, int ly, int lz, float *phi, const float *rho, const float *sigma,
+                  const uint8_t *type, float *H, const uint32_t *macro, int color, float damping) {
+    int64_t N = (int64_t)lx * ly * lz;
+    int mbx = (lx + MACRO_BLOCK - 1) / MACRO_BLOCK, mby = (ly + MACRO_BLOCK - 1) / MACRO_BLOCK;
+    for (int z = (color >> 2) & 1; z < lz; z += 2)
+        for (int y = (color >> 1) & 1; y < ly; y += 2)
+            for (int x = color & 1; x < lx; x += 2) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                int64_t mb = (x / MACRO_BLOCK) + (int64_t)mbx * ((y / MACRO_BLOCK) + (int64_t)mby * (z / MACRO_BLOCK));
+                float mres;
+                memcpy(&mres, &macro[mb], 4);
+                if (mres < 1e-4f) continue;
+                if (type[i] == 2 || type[i] == 0) { phi[i] = 0.0f; continue; }
+                float ss, sn, nphi6[6];
+                gs_accum(phi, sigma, N, i, x, y, z, lx, ly, lz, &ss, &sn, nphi6);
+                float phi_gs = (ss > 0.0f) ? (rho[i] + sn) / ss : 0.0f;
+                if (phi_gs > 0.0f) {
+                    float psi = amor_psi(sigma, N, i, nphi6, x, y, z, lx, ly, lz, phi_gs);
+                    H[i] = fmaxf(H[i], psi);
+                }
+                float result = clampf_(phi_gs, 0.0f, 1e7f);
+                if (damping > 0.0f) result *= damping;
+                if (isnan(result)) result = phi[i];
+                phi[i] = result;
+            }
+}
+
+void o_rbgs_step(int lx, int ly, int lz, float *phi, const float *rho, const float *sigma,
+                 const uint8_t *type, float *H, const uint32_t *macro, float damping) {
+    for (int c = 0; c < 8; c++) o_rbgs_color(lx, ly, lz, phi, rho, sigma, type, H, macro, c, damping);
+}
+
+/* ---- jacobi_smooth.comp.glsl:60-227 on a coarse level (omega = 1).
+ * phi_prev is a snapshot of phi taken before the pass (the reference binds
+ * the same buffer twice, which is a read/write race).  H is the FINE-level
+ * history buffer: the reference binds h_field_buf at every level
+ * (dispatcher_vcycle.cpp:178,287), so coarse cell i writes fine H[i]. ---- */
+void o_jacobi_coarse(int lx, int ly, int lz, float *phi, const float *phi_prev, const float *rho,
+                     const float *sigma, const uint8_t *type, float *Hfine, float damping) {
+    int64_t N = (int64_t)lx * ly * lz;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                if (type[i] == 2 || type[i] == 0) { phi[i] = 0.0f; continue; }
+                float ss, sn, nphi6[6];
+                gs_accum(phi_prev, sigma, N, i, x, y, z, lx, ly, lz, &ss, &sn, nphi6);
+                float phi_j = (ss > 0.0f) ? (rho[i] + sn) / ss : 1e7f;
+                float psi = amor_psi(sigma, N, i, nphi6, x, y, z, lx, ly, lz, phi_j);
+                Hfine[i] = fmaxf(Hfine[i], psi);
+                float prev = phi_prev[i];
+                float result = 1.0f * (phi_j - prev) + prev;
+                if (damping > 0.0f) result *= damping;
+                result = clampf_(result, 0.0f, 1e7f);
+                if (isnan(result)) result = prev;
+                phi[i] = result;
+            }
+}
+
+/* residual r = rho + L26 phi, mg_restrict.comp.glsl:53-116 */
+static float restrict_residual(const float *phi, const float *rho, const float *sigma, const uint8_t *type,
+                               int x, int y, int z, int lx, int ly, int lz) {
+    int64_t N = (int64_t)lx * ly * lz;
+    int64_t i = gidx(x, y, z, lx, ly);
+    if (type[i] != 1) return 0.0f;
+    int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+    float phi_i = phi[i], Lphi = 0.0f, s6[6];
+    for (int d = 0; d < 6; d++) s6[d] = sigma[(int64_t)d * N + i];
+    for (int d = 0; d < 6; d++)
+        if (valid[d] && s6[d] > 0.0f)
+            Lphi += s6[d] * (phi[gidx(x + OFS[d][0], y + OFS[d][1], z + OFS[d][2], lx, ly)] - phi_i);
+    for (int e = 0; e < 12; e++) {
+        if (!(valid[EDGE_DIRS[e][0]] && valid[EDGE_DIRS[e][1]])) continue;
+        float es = edge_w(s6, e);
+        const int *o = OFS[6 + e];
+        if (es > 0.0f) Lphi += es * (phi[gidx(x + o[0], y + o[1], z + o[2], lx, ly)] - phi_i);
+    }
+    for (int ci = 0; ci < 8; ci++) {
+        const int *o = OFS[18 + ci];
+        if (!inb(x + o[0], y + o[1], z + o[2], lx, ly, lz)) continue;
+        float cs = corner_w(s6, ci);
+        if (cs > 0.0f) Lphi += cs * (phi[gidx(x + o[0], y + o[1], z + o[2], lx, ly)] - phi_i);
+    }
+    return rho[i] + Lphi;
+}
+static float face_cond_sum(const float *sigma, int64_t N, int64_t i) {
+    float w = 0.0f;
+    for (int d = 0; d < 6; d++) {
+        float s = sigma[(int64_t)d * N + i];
+        if (s > 0.0f) w += s;
+    }
+    return w;
+}
+
+/* ---- mg_restrict.comp.glsl:118-195 ---- */
+void o_restrict(int fx_, int fy_, int fz_, const float *phi_f, const float *rho_f, const float *sig_f,
+                const uint8_t *type_f, int cx_, int cy_, int cz_, float *phi_c, float *rho_c) {
+    int64_t Nf = (int64_t)fx_ * fy_ * fz_;
+    for (int cz = 0; cz < cz_; cz++)
+        for (int cy = 0; cy < cy_; cy++)
+            for (int cx = 0; cx < cx_; cx++) {
+                int64_t c = gidx(cx, cy, cz, cx_, cy_);
+                float swr = 0.0f, tw = 0.0f, sur = 0.0f;
+                int count = 0;
+                for (int dz = 0; dz < 2; dz++)
+                    for (int dy = 0; dy < 2; dy++)
+                        for (int dx = 0; dx < 2; dx++) {
+                            int x = cx * 2 + dx, y = cy * 2 + dy, z = cz * 2 + dz;
+                            if (x < fx_ && y < fy_ && z < fz_) {
+                                float r = restrict_residual(phi_f, rho_f, sig_f, type_f, x, y, z, fx_, fy_, fz_);
+                                float w = face_cond_sum(sig_f, Nf, gidx(x, y, z, fx_, fy_));
+                                swr += w * r; tw += w; sur += r; count++;
+                            }
+                        }
+                if (tw > 1e-20f) rho_c[c] = (swr / tw) * (float)count;
+                else rho_c[c] = (count > 0) ? sur : 0.0f;
+                float swp = 0.0f, tpw = 0.0f, sp = 0.0f;
+                count = 0;
+                for (int dz = 0; dz < 2; dz++)
+                    for (int dy = 0; dy < 2; dy++)
+                        for (int dx = 0; dx < 2; dx++) {
+                            int x = cx * 2 + dx, y = cy * 2 + dy, z = cz * 2 + dz;
+                            if (x < fx_ && y < fy_ && z < fz_) {
+                                int64_t i = gidx(x, y, z, fx_, fy_);
+                                float p = phi_f[i], w = face_cond_sum(sig_f, Nf, i);
+                                swp += w * p; tpw += w; sp += p; count++;
+                            }
+                        }
+                if (tpw > 1e-20f) phi_c[c] = swp / tpw;
+                else phi_c[c] = (count > 0) ? sp / (float)count : 0.0f;
+            }
+}
+
+/* ---- mg_prolong.comp.glsl:233-275 ---- */
+void o_prolong(int fx_, int fy_, int fz_, float *phi_f, int cx_, int cy_, int cz_, const float *phi_c) {
+    for (int z = 0; z < fz_; z++)
+        for (int y = 0; y < fy_; y++)
+            for (int x = 0; x < fx_; x++) {
+                float cxf = (float)x * 0.5f, cyf = (float)y * 0.5f, czf = (float)z * 0.5f;
+                int x0 = (int)floorf(cxf), y0 = (int)floorf(cyf), z0 = (int)floorf(czf);
+                float wx = cxf - (float)x0, wy = cyf - (float)y0, wz = czf - (float)z0;
+                float c[2][2][2];
+                for (int k = 0; k < 2; k++)
+                    for (int j = 0; j < 2; j++)
+                        for (int ii = 0; ii < 2; ii++) {
+                            int ax = x0 + ii, ay = y0 + j, az = z0 + k;
+                            ax = ax < 0 ? 0 : (ax > cx_ - 1 ? cx_ - 1 : ax);
+                            ay = ay < 0 ? 0 : (ay > cy_ - 1 ? cy_ - 1 : ay);
+                            az = az < 0 ? 0 : (az > cz_ - 1 ? cz_ - 1 : az);
+                            c[k][j][ii] = phi_c[gidx(ax, ay, az, cx_, cy_)];
+                        }
+                /* GLSL mix(a,b,t) = a*(1-t) + b*t */
+#define MIX(a, b, t) ((a) * (1.0f - (t)) + (b) * (t))
+                float corr = MIX(MIX(MIX(c[0][0][0], c[0][0][1], wx), MIX(c[0][1][0], c[0][1][1], wx), wy),
+                                 MIX(MIX(c[1][0][0], c[1][0][1], wx), MIX(c[1][1][0], c[1][1][1], wx), wy), wz);
+#undef MIX
+                phi_f[gidx(x, y, z, fx_, fy_)] += corr;
+            }
+}
+
+/* ---- island_buffer.cpp:600-700 downsampleLevel ---- */
+void o_downsample(int sx, int sy, int sz, const float *src_cond, const uint8_t *src_type,
+                  int dx_, int dy_, int dz_, float *out_cond, uint8_t *out_type) {
+    int64_t sN = (int64_t)sx * sy * sz, dN = (int64_t)dx_ * dy_ * dz_;
+    for (int cz = 0; cz < dz_; cz++)
+        for (int cy = 0; cy < dy_; cy++)
+            for (int cx = 0; cx < dx_; cx++) {
+                int64_t ci = gidx(cx, cy, cz, dx_, dy_);
+                float sum[6] = {0, 0, 0, 0, 0, 0};
+                int contrib = 0, solid = 0, anchor = 0;
+                for (int ddz = 0; ddz < 2 && cz * 2 + ddz < sz; ddz++)
+                    for (int ddy = 0; ddy < 2 && cy * 2 + ddy < sy; ddy++)
+                        for (int ddx = 0; ddx < 2 && cx * 2 + ddx < sx; ddx++) {
+                            int64_t fi = gidx(cx * 2 + ddx, cy * 2 + ddy, cz * 2 + ddz, sx, sy);
+                            contrib++;
+                            uint8_t t = src_type[fi];
+                            if (t == 2) anchor++;
+                            else if (t == 1) solid++;
+                            for (int d = 0; d < 6; d++) sum[d] += src_cond[(int64_t)d * sN + fi];
+                        }
+                for (int d = 0; d < 6; d++) out_cond[(int64_t)d * dN + ci] = 0.0f;
+                if (contrib > 0) {
+                    float inv = 1.0f / (float)contrib;
+                    for (int d = 0; d < 6; d++) out_cond[(int64_t)d * dN + ci] = sum[d] * inv;
+                }
+                out_type[ci] = anchor > 0 ? 2 : (solid > contrib / 2 ? 1 : 0);
+            }
+}
+
+/* ---- PCG kernels ---- */
+static float diag26_valid(const float *sigma, int64_t N, int64_t i, int x, int y, int z, int lx, int ly, int lz) {
+    int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+    float s6[6], diag = 0.0f;
+    for (int d = 0; d < 6; d++) s6[d] = sigma[(int64_t)d * N + i];
+    for (int d = 0; d < 6; d++) if (valid[d] && s6[d] > 0.0f) diag += s6[d];
+    for (int e = 0; e < 12; e++)
+        if (valid[EDGE_DIRS[e][0]] && valid[EDGE_DIRS[e][1]]) diag += edge_w(s6, e);
+    for (int ci = 0; ci < 8; ci++) {
+        const int *o = OFS[18 + ci];
+        if (!inb(x + o[0], y + o[1], z + o[2], lx, ly, lz)) continue;
+        diag += corner_w(s6, ci);
+    }
+    return diag;
+}
+
+/* pcg_precompute.comp.glsl:24-86 -- note the 6 faces are summed without a
+ * bounds check while edges and corners are bounds-checked. */
+void o_pcg_precompute(int lx, int ly, int lz, const float *sigma, float *invdiag) {
+    int64_t N = (int64_t)lx * ly * lz;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+                float s6[6];
+                for (int d = 0; d < 6; d++) s6[d] = sigma[(int64_t)d * N + i];
+                float d26 = s6[0] + s6[1] + s6[2] + s6[3] + s6[4] + s6[5];
+                for (int e = 0; e < 12; e++)
+                    if (valid[EDGE_DIRS[e][0]] && valid[EDGE_DIRS[e][1]]) d26 += edge_w(s6, e);
+                for (int ci = 0; ci < 8; ci++) {
+                    const int *o = OFS[18 + ci];
+                    if (!inb(x + o[0], y + o[1], z + o[2], lx, ly, lz)) continue;
+                    d26 += corner_w(s6, ci);
+                }
+                invdiag[i] = (d26 > 1e-20f) ? (1.0f / d26) : 0.0f;
+            }
+}
+
+/* pcg_matvec.comp.glsl:128-214 -- out = sum_j w_ij (in_i - in_j) */
+void o_pcg_matvec(int lx, int ly, int lz, const float *in, float *out, const float *sigma, const uint8_t *type) {
+    int64_t N = (int64_t)lx * ly * lz;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                if (type[i] == 0 || type[i] == 2) { out[i] = 0.0f; continue; }
+                int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+                float c = in[i], res = 0.0f, s6[6];
+                for (int d = 0; d < 6; d++) s6[d] = sigma[(int64_t)d * N + i];
+                for (int d = 0; d < 6; d++) {
+                    if (!valid[d]) continue;
+                    if (s6[d] > 0.0f) {
+                        float nv = in[gidx(x + OFS[d][0], y + OFS[d][1], z + OFS[d][2], lx, ly)];
+                        if (finitef_(nv)) res += s6[d] * (c - nv);
+                    }
+                }
+                for (int e = 0; e < 12; e++) {
+                    if (!(valid[EDGE_DIRS[e][0]] && valid[EDGE_DIRS[e][1]])) continue;
+                    float es = edge_w(s6, e);
+                    if (es > 0.0f) {
+                        const int *o = OFS[6 + e];
+                        float ep = in[gidx(x + o[0], y + o[1], z + o[2], lx, ly)];
+                        if (finitef_(ep)) res += es * (c - ep);
+                    }
+                }
+                for (int ci = 0; ci < 8; ci++) {
+                    const int *o = OFS[18 + ci];
+                    if (!inb(x + o[0], y + o[1], z + o[2], lx, ly, lz)) continue;
+                    float cs = corner_w(s6, ci);
+                    if (cs > 0.0f) {
+                        float cp = in[gidx(x + o[0], y + o[1], z + o[2], lx, ly)];
+                        if (finitef_(cp)) res += cs * (c - cp);
+                    }
+                }
+                if (!finitef_(res)) res = 0.0f;
+                out[i] = res;
+            }
+}
+
+/* Sum of r*z over the voxels whose pcg_update partial lands in the
+ * ceil(N/512)-entry partial buffer: workgroups of 256 voxels write
+ * partialSums[wg] but pass 2 reduces only ceil(N/512) entries
+ * (dispatcher_pcg.cpp:254-298, island_buffer.cpp allocatePCG), so the sum
+ * covers voxels [0, min(N, 256*ceil(N/512))). */
+int64_t o_rtz_limit(int64_t N) {
+    int64_t g = (N + 511) / 512;
+    int64_t m = 256 * g;
+    return m < N ? m : N;
+}
+
+/* pcg_update.comp.glsl:116-211.  Returns the partial-range r.z sum (FP64
+ * accumulation of FP32 products; the GPU reduces the same products in FP32
+ * with a tree).  r_prev: r as it was before this dispatch (SSOR-correction
+ * source). */
+double o_pcg_update(int lx, int ly, int lz, float *phi, float *r, const float *r_prev, float *p, const float *ap,
+                    const float *src, const uint8_t *type, const float *sigma, const float *invdiag,
+                    const float *red, int is_init) {
+    int64_t N = (int64_t)lx * ly * lz, lim = o_rtz_limit(N);
+    double acc = 0.0;
+    int64_t LxLy = (int64_t)lx * ly;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+                float rz = 0.0f;
+                if (is_init) {
+                    if (type[i] == 1) {
+                        float ri = src[i] - ap[i];
+                        if (!finitef_(ri)) ri = 0.0f;
+                        r[i] = ri;
+                        float diag = diag26_valid(sigma, N, i, x, y, z, lx, ly, lz);
+                        float zi = (diag > 1e-20f) ? ri / diag : ri;
+                        if (!finitef_(zi)) zi = 0.0f;
+                        p[i] = zi;
+                        rz = ri * zi;
+                    } else {
+                        r[i] = 0.0f;
+                        p[i] = 0.0f;
+                    }
+                } else if (type[i] == 1) {
+                    float rTz_old = red[0], pAp = red[1];
+                    float alpha = (pAp > 1e-30f) ? rTz_old / pAp : 0.0f;
+                    float corr = 0.0f;
+                    int64_t nb[6] = {i - 1, i + 1, i - lx, i + lx, i - LxLy, i + LxLy};
+                    for (int d = 0; d < 6; d++)
+                        if (valid[d]) corr += sigma[(int64_t)d * N + i] * (r_prev[nb[d]] * invdiag[nb[d]]);
+                    float ph = phi[i] + alpha * p[i];
+                    r[i] = r_prev[i] - alpha * ap[i];
+                    ph = clampf_(ph, 0.0f, 1e7f);
+                    if (isnan(ph)) ph = 0.0f;
+                    phi[i] = ph;
+                    float ri = r[i];
+                    if (!finitef_(ri)) { ri = 0.0f; r[i] = 0.0f; }
+                    float diag = diag26_valid(sigma, N, i, x, y, z, lx, ly, lz);
+                    float zj = (diag > 1e-20f) ? ri / diag : ri;
+                    float zi = zj + ((diag > 1e-20f) ? corr / diag : 0.0f);
+                    if (!finitef_(zi)) zi = zj;
+                    rz = ri * zi;
+                }
+                if (i < lim) acc += (double)rz;
+            }
+    return acc;
+}
+
+/* pcg_direction.comp.glsl:336-379 */
+void o_pcg_direction(int lx, int ly, int lz, const float *r, float *p, const uint8_t *type, const float *red,
+                     const float *sigma) {
+    int64_t N = (int64_t)lx * ly * lz, LxLy = (int64_t)lx * ly;
+    float rTz_old = red[0], rTz_new = red[2];
+    float beta = (rTz_old > 1e-30f) ? rTz_new / rTz_old : 0.0f;
+    beta = clampf_(beta, 0.0f, 10.0f);
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                if (type[i] != 1) { p[i] = 0.0f; continue; }
+                int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+                float ri = r[i];
+                float diag = diag26_valid(sigma, N, i, x, y, z, lx, ly, lz);
+                int64_t nb[6] = {i - 1, i + 1, i - lx, i + lx, i - LxLy, i + LxLy};
+                float corr = 0.0f;
+                for (int d = 0; d < 6; d++) {
+                    if (!valid[d]) continue;
+                    int64_t j = nb[d];
+                    float rj = r[j];
+                    float d6j = sigma[0 * N + j] + sigma[1 * N + j] + sigma[2 * N + j] + sigma[3 * N + j] +
+                                sigma[4 * N + j] + sigma[5 * N + j];
+                    corr += sigma[(int64_t)d * N + i] * ((d6j > 1e-20f) ? rj / d6j : 0.0f);
+                }
+                float zj = (diag > 1e-20f) ? ri / diag : ri;
+                float zi = zj + ((diag > 1e-20f) ? corr / diag : 0.0f);
+                if (!finitef_(zi)) zi = zj;
+                float np = zi + beta * p[i];
+                if (!finitef_(np)) np = zi;
+                p[i] = np;
+            }
+}
+
+double o_dot(int64_t n, const float *a, const float *b) {
+    double acc = 0.0;
+    for (int64_t i = 0; i < n; i++) acc += (double)(a[i] * b[i]);
+    return acc;
+}
+
+/* ---- phase_field_evolve.comp.glsl:246-364 ---- */
+void o_phase_field(int lx, int ly, int lz, const float *phi, const float *H, float *D, const float *sigma,
+                   const uint8_t *type, uint32_t *fail, const float *hyd, float l0, float gc, float relax,
+                   int split) {
+    int64_t N = (int64_t)lx * ly * lz;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                if (type[i] == 0 || type[i] == 2) continue;
+                if (fail[i] != 0) continue;
+                float phi_i = phi[i], sumSigma = 0.0f, lap_phi = 0.0f, lap_d = 0.0f, d_i = D[i];
+                for (int d = 0; d < 6; d++) {
+                    int nx = x + OFS[d][0], ny = y + OFS[d][1], nz = z + OFS[d][2];
+                    if (!inb(nx, ny, nz, lx, ly, lz)) continue;
+                    int64_t j = gidx(nx, ny, nz, lx, ly);
+                    if (type[j] == 0) continue;
+                    float s = sigma[(int64_t)d * N + i], pj = phi[j], dj = D[j];
+                    if (finitef_(pj)) { lap_phi += (pj - phi_i); sumSigma += s; }
+                    if (finitef_(dj)) lap_d += (dj - d_i);
+                }
+                float Hv = H[i];
+                if (Hv <= 0.0f) continue;
+                float hdeg = clampf_(hyd[i], 0.01f, 1.0f);
+                float gce = gc * powf(hdeg, 1.5f);
+                float Heff = Hv;
+                if (split) {
+                    float sd = fmaxf(sumSigma, 1e-12f);
+                    float fo = fmaxf(lap_phi, 0.0f);
+                    Heff = fmaxf(Hv, fo / sd);
+                }
+                float num = 2.0f * Heff + gce * l0 * lap_d;
+                float den = 2.0f * Heff + gce / l0;
+                den = fmaxf(den, 1e-8f);
+                float dn = clampf_(num / den, d_i, 1.0f);
+                dn = d_i * (1.0f - relax) + dn * relax;
+                dn = clampf_(dn, 0.0f, 1.0f);
+                if (!finitef_(dn)) dn = d_i;
+                D[i] = dn;
+                if (dn > 0.95f) fail[i] = 1;
+            }
+}
+
+/* ---- failure_scan.comp.glsl:36-196 ---- */
+void o_failure_scan(int lx, int ly, int lz, const float *phi, const float *sigma, const float *maxphi,
+                    const float *rcomp, const uint8_t *type, uint32_t *fail, const float *rtens, uint32_t *macro,
+                    const float *rho, float phi_orphan) {
+    int64_t N = (int64_t)lx * ly * lz;
+    int mbx = (lx + MACRO_BLOCK - 1) / MACRO_BLOCK, mby = (ly + MACRO_BLOCK - 1) / MACRO_BLOCK;
+    (void)maxphi;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                fail[i] = 0;
+                if (type[i] != 1) continue;
+                float p = phi[i], s6[6];
+                for (int d = 0; d < 6; d++) s6[d] = sigma[(int64_t)d * N + i];
+                float sum6 = s6[0] + s6[1] + s6[2] + s6[3] + s6[4] + s6[5];
+                if (sum6 == 0.0f || p > phi_orphan) { fail[i] = 3; continue; }
+                int valid[6] = {x > 0, x + 1 < lx, y > 0, y + 1 < ly, z > 0, z + 1 < lz};
+                float fin = 0.0f, fout = 0.0f;
+                for (int d = 0; d < 6; d++) {
+                    if (!valid[d]) continue;
+                    if (s6[d] > 0.0f) {
+                        float dphi = phi[gidx(x + OFS[d][0], y + OFS[d][1], z + OFS[d][2], lx, ly)] - p;
+                        if (dphi > 0.0f) fin += s6[d] * dphi;
+                        else if (dphi < 0.0f) fout += s6[d] * (-dphi);
+                    }
+                }
+                float sxa = (s6[0] + s6[1]) * 0.5f, sya = (s6[2] + s6[3]) * 0.5f, sza = (s6[4] + s6[5]) * 0.5f;
+                float ew[3] = {sqrtf(fmaxf(sxa * sya, 0.0f)) * EDGE_P, sqrtf(fmaxf(sxa * sza, 0.0f)) * EDGE_P,
+                               sqrtf(fmaxf(sya * sza, 0.0f)) * EDGE_P};
+                for (int plane = 0; plane < 3; plane++) {
+                    if (!(ew[plane] > 0.0f)) continue;
+                    for (int k = 0; k < 4; k++) {
+                        int e = plane * 4 + k;
+                        if (!(valid[EDGE_DIRS[e][0]] && valid[EDGE_DIRS[e][1]])) continue;
+                        const int *o = OFS[6 + e];
+                        float dphi = phi[gidx(x + o[0], y + o[1], z + o[2], lx, ly)] - p;
+                        if (dphi > 0.0f) fin += ew[plane] * dphi;
+                        else fout += ew[plane] * (-dphi);
+                    }
+                }
+                float cw = cbrtf(fmaxf(sxa * sya * sza, 0.0f)) * CORNER_P;
+                if (cw > 0.0f) {
+                    for (int ci = 0; ci < 8; ci++) {
+                        const int *o = OFS[18 + ci];
+                        if (!inb(x + o[0], y + o[1], z + o[2], lx, ly, lz)) continue;
+                        float dphi = phi[gidx(x + o[0], y + o[1], z + o[2], lx, ly)] - p;
+                        if (dphi > 0.0f) fin += cw * dphi;
+                        else fout += cw * (-dphi);
+                    }
+                }
+                if (rcomp[i] > 0.0f && fin > rcomp[i]) { fail[i] = 2; continue; }
+                if (rtens[i] > 0.0f && fout > rtens[i]) { fail[i] = 4; continue; }
+                float res = fabsf(fin - fout + rho[i]);
+                int64_t mb = (x / MACRO_BLOCK) + (int64_t)mbx * ((y / MACRO_BLOCK) + (int64_t)mby * (z / MACRO_BLOCK));
+                uint32_t bits;
+                memcpy(&bits, &res, 4);
+                if (bits > macro[mb]) macro[mb] = bits;
+            }
+}
+
+/* ============================ island state ============================ */
+typedef struct {
+    int32_t lx, ly, lz;
+    int64_t n, nmb;
+    float *phi, *src, *sigma, *rcomp, *rtens, *maxphi, *hyd, *H, *D;
+    uint8_t *type;
+    uint32_t *fail, *macro;
+    /* multigrid */
+    int32_t mg_alloc, l1[3], l2[3];
+    int64_t n1, n2;
+    float *phi1, *src1, *sig1, *phi2, *src2, *sig2, *snap;
+    uint8_t *type1, *type2;
+    /* pcg */
+    int32_t pcg_alloc;
+    float *r, *rprev, *p, *ap, *invdiag;
+    float red[4];
+    /* schedule state */
+    int32_t chebyshev_iter, pcg_enabled, phase_field;
+    float prev_macro, last_macro;
+} pfo_island;
+
+pfo_island *pfo_create(int lx, int ly, int lz) {
+    pfo_island *s = (pfo_island *)calloc(1, sizeof(pfo_island));
+    s->lx = lx; s->ly = ly; s->lz = lz;
+    s->n = (int64_t)lx * ly * lz;
+    int64_t n = s->n;
+    s->nmb = (int64_t)((lx + 7) / 8) * ((ly + 7) / 8) * ((lz + 7) / 8);
+    s->phi = calloc(n, 4); s->src = calloc(n, 4); s->sigma = calloc(6 * n, 4);
+    s->rcomp = calloc(n, 4); s->rtens = calloc(n, 4); s->maxphi = calloc(n, 4);
+    s->hyd = calloc(n, 4); s->H = calloc(n, 4); s->D = calloc(n, 4);
+    s->type = calloc(n, 1); s->fail = calloc(n, 4); s->macro = calloc(s->nmb > 0 ? s->nmb : 1, 4);
+    for (int64_t i = 0; i < n; i++) s->hyd[i] = 1.0f; /* island_buffer.cpp: hydration filled with 1.0f */
+    s->pcg_enabled = 1;
+    s->phase_field = 1;
+    return s;
+}
+void pfo_destroy(pfo_island *s) {
+    if (!s) return;
+    void *ptrs[] = {s->phi, s->src, s->sigma, s->rcomp, s->rtens, s->maxphi, s->hyd, s->H, s->D, s->type,
+                    s->fail, s->macro, s->phi1, s->src1, s->sig1, s->phi2, s->src2, s->sig2, s->snap,
+                    s->type1, s->type2, s->r, s->rprev, s->p, s->ap, s->invdiag};
+    for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
+    free(s);
+}
+/* accessors for ctypes */
+void *pfo_ptr(pfo_island *s, int which) {
+    switch (which) {
+    case 0: return s->phi; case 1: return s->src; case 2: return s->sigma; case 3: return s->type;
+    case 4: return s->rcomp; case 5: return s->rtens; case 6: return s->maxphi; case 7: return s->hyd;
+    case 8: return s->H; case 9: return s->D; case 10: return s->fail; case 11: return s->macro;
+    case 12: return s->red;
+    default: return NULL;
+    }
+}
+void pfo_get_state(pfo_island *s, int32_t *iout, float *fout) {
+    iout[0] = s->chebyshev_iter; iout[1] = s->pcg_alloc; iout[2] = s->mg_alloc;
+    fout[0] = s->prev_macro; fout[1] = s->last_macro;
+}
+void pfo_set_flags(pfo_island *s, int pcg_enabled, int phase_field) {
+    s->pcg_enabled = pcg_enabled; s->phase_field = phase_field;
+}
+
+static void mg_alloc(pfo_island *s) {
+    if (s->mg_alloc) return;
+    s->l1[0] = (s->lx + 1) / 2; s->l1[1] = (s->ly + 1) / 2; s->l1[2] = (s->lz + 1) / 2;
+    s->l2[0] = (s->l1[0] + 1) / 2; s->l2[1] = (s->l1[1] + 1) / 2; s->l2[2] = (s->l1[2] + 1) / 2;
+    s->n1 = (int64_t)s->l1[0] * s->l1[1] * s->l1[2];
+    s->n2 = (int64_t)s->l2[0] * s->l2[1] * s->l2[2];
+    s->phi1 = calloc(s->n1, 4); s->src1 = calloc(s->n1, 4); s->sig1 = calloc(6 * s->n1, 4); s->type1 = calloc(s->n1, 1);
+    s->phi2 = calloc(s->n2, 4); s->src2 = calloc(s->n2, 4); s->sig2 = calloc(6 * s->n2, 4); s->type2 = calloc(s->n2, 1);
+    s->snap = calloc(s->n1, 4);
+    s->mg_alloc = 1;
+}
+static void mg_upload(pfo_island *s) {
+    o_downsample(s->lx, s->ly, s->lz, s->sigma, s->type, s->l1[0], s->l1[1], s->l1[2], s->sig1, s->type1);
+    if (s->n2 > 0)
+        o_downsample(s->l1[0], s->l1[1], s->l1[2], s->sig1, s->type1, s->l2[0], s->l2[1], s->l2[2], s->sig2, s->type2);
+}
+static void pcg_alloc(pfo_island *s) {
+    if (s->pcg_alloc) return;
+    s->r = calloc(s->n, 4); s->rprev = calloc(s->n, 4); s->p = calloc(s->n, 4);
+    s->ap = calloc(s->n, 4); s->invdiag = calloc(s->n, 4);
+    s->pcg_alloc = 1;
+}
+
+static float damping_of(int it) { return it >= WARMUP_STEPS ? DAMPING_FACTOR : 0.0f; }
+
+static void coarse_pass(pfo_island *s, int lvl, float damping) {
+    int *L = lvl == 1 ? s->l1 : s->l2;
+    int64_t n = lvl == 1 ? s->n1 : s->n2;
+    float *ph = lvl == 1 ? s->phi1 : s->phi2;
+    memcpy(s->snap, ph, n * 4);
+    o_jacobi_coarse(L[0], L[1], L[2], ph, s->snap, lvl == 1 ? s->src1 : s->src2, lvl == 1 ? s->sig1 : s->sig2,
+                    lvl == 1 ? s->type1 : s->type2, s->H, damping);
+}
+
+/* dispatcher_vcycle.cpp:342-392 */
+static int vcycle(pfo_island *s) {
+    float damping = damping_of(s->chebyshev_iter);
+    o_rbgs_step(s->lx, s->ly, s->lz, s->phi, s->src, s->sigma, s->type, s->H, s->macro, damping);
+    s->chebyshev_iter++;
+    o_restrict(s->lx, s->ly, s->lz, s->phi, s->src, s->sigma, s->type, s->l1[0], s->l1[1], s->l1[2], s->phi1, s->src1);
+    if (s->n2 > 0) {
+        for (int leg = 0; leg < 2; leg++) {
+            coarse_pass(s, 1, damping); coarse_pass(s, 1, damping);
+            o_restrict(s->l1[0], s->l1[1], s->l1[2], s->phi1, s->src1, s->sig1, s->type1, s->l2[0], s->l2[1],
+                       s->l2[2], s->phi2, s->src2);
+            for (int k = 0; k < 4; k++) coarse_pass(s, 2, damping);
+            o_prolong(s->l1[0], s->l1[1], s->l1[2], s->phi1, s->l2[0], s->l2[1], s->l2[2], s->phi2);
+            coarse_pass(s, 1, damping); coarse_pass(s, 1, damping);
+        }
+    } else {
+        for (int k = 0; k < 4; k++) coarse_pass(s, 1, damping);
+    }
+    o_prolong(s->lx, s->ly, s->lz, s->phi, s->l1[0], s->l1[1], s->l1[2], s->phi1);
+    o_rbgs_step(s->lx, s->ly, s->lz, s->phi, s->src, s->sigma, s->type, s->H, s->macro, damping);
+    s->chebyshev_iter++;
+    return 2;
+}
+
+static int mg_interval(const pfo_island *s) {
+    int mx = s->lx > s->ly ? (s->lx > s->lz ? s->lx : s->lz) : (s->ly > s->lz ? s->ly : s->lz);
+    int mn = s->lx < s->ly ? (s->lx < s->lz ? s->lx : s->lz) : (s->ly < s->lz ? s->ly : s->lz);
+    if (mn <= 0) return MG_INTERVAL;
+    int ratio = mx / mn;
+    if (ratio >= 8) return 1;
+    if (ratio >= 4) return 2;
+    return MG_INTERVAL;
+}
+
+/* dispatcher.cpp:188-238; mg_coarse_dirty is always set on a dirty tick
+ * because uploadFromHosts runs first (island_buffer.cpp:588). */
+static int try_vcycle(pfo_island *s, int k, int mg_available, int *mg_dirty) {
+    int interval = mg_interval(s);
+    if (!(k > 0 && (k % interval) == 0 && mg_available)) return 0;
+    if (!s->mg_alloc) { mg_alloc(s); mg_upload(s); *mg_dirty = 0; }
+    else if (*mg_dirty) { mg_upload(s); *mg_dirty = 0; }
+    vcycle(s);
+    int mx = s->lx > s->ly ? (s->lx > s->lz ? s->lx : s->lz) : (s->ly > s->lz ? s->ly : s->lz);
+    int mn = s->lx < s->ly ? (s->lx < s->lz ? s->lx : s->lz) : (s->ly < s->lz ? s->ly : s->lz);
+    if (mn > 0 && mx >= 8 * mn) vcycle(s);
+    return 1;
+}
+
+static void pcg_initial(pfo_island *s) {
+    o_pcg_precompute(s->lx, s->ly, s->lz, s->sigma, s->invdiag);
+    o_pcg_matvec(s->lx, s->ly, s->lz, s->phi, s->ap, s->sigma, s->type);
+    double rz = o_pcg_update(s->lx, s->ly, s->lz, s->phi, s->r, s->r, s->p, s->ap, s->src, s->type, s->sigma,
+                             s->invdiag, s->red, 1);
+    s->red[0] = (float)rz;
+}
+static void pcg_step(pfo_island *s) {
+    o_pcg_matvec(s->lx, s->ly, s->lz, s->p, s->ap, s->sigma, s->type);
+    s->red[1] = (float)o_dot(s->n, s->p, s->ap);
+    memcpy(s->rprev, s->r, s->n * 4);
+    double rz = o_pcg_update(s->lx, s->ly, s->lz, s->phi, s->r, s->rprev, s->p, s->ap, s->src, s->type, s->sigma,
+                             s->invdiag, s->red, 0);
+    s->red[2] = (float)rz;
+    o_pcg_direction(s->lx, s->ly, s->lz, s->r, s->p, s->type, s->red, s->sigma);
+    s->red[0] = s->red[2];
+}
+
+/* dispatcher.cpp:106-186.  Returns the number of counted steps. */
+int o_solve_steps(pfo_island *s, int steps) {
+    int recorded = 0, mg_dirty = 1;
+    int mx = s->lx > s->ly ? (s->lx > s->lz ? s->lx : s->lz) : (s->ly > s->lz ? s->ly : s->lz);
+    int mg_available = mx > 4;
+    if (steps >= PCG_MIN_RBGS + PCG_MIN_STEPS) {
+        float prev = s->prev_macro, curr = s->last_macro;
+        float ratio = (prev > 1e-10f) ? (curr / prev) : 0.0f;
+        int stalled = ratio > 0.95f;
+        if (stalled && s->pcg_enabled && !s->pcg_alloc) pcg_alloc(s);
+        int supports = s->pcg_enabled && s->n <= PCG_MAX_N && s->pcg_alloc;
+        if (supports) {
+            int maxr = steps - PCG_MIN_STEPS > PCG_MIN_RBGS ? steps - PCG_MIN_STEPS : PCG_MIN_RBGS;
+            int rb = stalled ? PCG_MIN_RBGS : maxr;
+            int pc = steps - rb;
+            for (int k = 0; k < rb; k++) {
+                if (try_vcycle(s, k, mg_available, &mg_dirty)) continue;
+                o_rbgs_step(s->lx, s->ly, s->lz, s->phi, s->src, s->sigma, s->type, s->H, s->macro,
+                            damping_of(s->chebyshev_iter));
+                s->chebyshev_iter++;
+                recorded++;
+            }
+            pcg_initial(s);
+            for (int k = 0; k < pc; k++) { pcg_step(s); recorded++; }
+            return recorded;
+        }
+    }
+    for (int k = 0; k < steps; k++) {
+        if (try_vcycle(s, k, mg_available, &mg_dirty)) continue;
+        o_rbgs_step(s->lx, s->ly, s->lz, s->phi, s->src, s->sigma, s->type, s->H, s->macro,
+                    damping_of(s->chebyshev_iter));
+        s->chebyshev_iter++;
+        recorded++;
+    }
+    return recorded;
+}
+
+/* One dirty-island tick: pfsf_engine.cpp:470-513 (without the host
+ * upload, which the caller does by writing the input arrays). */
+void o_tick(pfo_island *s) {
+    for (int64_t b = 0; b < s->nmb; b++) s->macro[b] = MACRO_SEED_BITS;
+    o_solve_steps(s, STEPS_MAJOR);
+    if (s->phase_field)
+        o_phase_field(s->lx, s->ly, s->lz, s->phi, s->H, s->D, s->sigma, s->type, s->fail, s->hyd, PF_L0, PF_GC,
+                      PF_RELAX, 1);
+    o_failure_scan(s->lx, s->ly, s->lz, s->phi, s->sigma, s->maxphi, s->rcomp, s->type, s->fail, s->rtens, s->macro,
+                   s->src, PHI_ORPHAN);
+    float mx = 0.0f;
+    for (int64_t b = 0; b < s->nmb; b++) {
+        float f;
+        memcpy(&f, &s->macro[b], 4);
+        if (f > mx) mx = f;
+    }
+    s->prev_macro = s->last_macro;
+    s->last_macro = mx;
+}
+
+/* island_buffer.cpp:864-966: append {x,y,z,type} (world coords) of every
+ * non-zero fail flag in index order after the count already in the
+ * header, up to the DBB capacity. */
+int32_t o_readback_failures(const pfo_island *s, int32_t ox, int32_t oy, int32_t oz, void *dbb, int64_t bytes) {
+    if (!dbb || bytes < 20) return -1;
+    int32_t *hdr = (int32_t *)dbb;
+    int32_t count = *hdr;
+    int32_t cap = (int32_t)((bytes - 4) / 16);
+    int32_t *t = hdr + 1;
+    for (int64_t idx = 0; idx < s->n && count < cap; idx++) {
+        uint32_t f = s->fail[idx];
+        if (f == 0) continue;
+        t[count * 4 + 0] = ox + (int32_t)(idx % s->lx);
+        t[count * 4 + 1] = oy + (int32_t)((idx / s->lx) % s->ly);
+        t[count * 4 + 2] = oz + (int32_t)(idx / ((int64_t)s->lx * s->ly));
+        t[count * 4 + 3] = (int32_t)f;
+        count++;
+    }
+    *hdr = count;
+    return count;
+}
+
+/* ======================= symmetric kappa operator ======================= */
+/* Link weight between 26-neighbours i and j (both non-air):
+ *   w_ij = c_k * 2 k_i k_j / (k_i + k_j),  c = 1 (face), 0.5 (edge), 1/6 (corner).
+ * Unknowns are SOLID voxels; ANCHOR voxels are Dirichlet (phi = 0); AIR and
+ * out-of-box links are dropped.  Row i (solid):  sum_j w_ij (phi_i - phi_j) = s_i.
+ * Same symmetric per-link structure as the reference's CPU solver
+ * (Block Reality/api/src/test/java/com/blockreality/api/physics/validation/
+ * VoxelPhysicsCpuReference.java:84-113), with the harmonic-mean link
+ * conductivity the benchmark configurations specify. */
+static const double KC[26] = {1, 1, 1, 1, 1, 1, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5,
+                              1.0 / 6, 1.0 / 6, 1.0 / 6, 1.0 / 6, 1.0 / 6, 1.0 / 6, 1.0 / 6, 1.0 / 6};
+
+static double hm(double a, double b) { return (a + b) > 0.0 ? 2.0 * a * b / (a + b) : 0.0; }
+
+/* y = A x over solid rows (other rows 0); FP64. */
+void o_kappa_apply(int lx, int ly, int lz, const double *kappa, const uint8_t *type, const double *x, double *y) {
+    for (int z = 0; z < lz; z++)
+        for (int yy = 0; yy < ly; yy++)
+            for (int xx = 0; xx < lx; xx++) {
+                int64_t i = gidx(xx, yy, z, lx, ly);
+                if (type[i] != 1) { y[i] = 0.0; continue; }
+                double acc = 0.0, xi = x[i];
+                for (int k = 0; k < 26; k++) {
+                    int nx = xx + OFS[k][0], ny = yy + OFS[k][1], nz = z + OFS[k][2];
+                    if (!inb(nx, ny, nz, lx, ly, lz)) continue;
+                    int64_t j = gidx(nx, ny, nz, lx, ly);
+                    if (type[j] == 0) continue;
+                    double w = KC[k] * hm(kappa[i], kappa[j]);
+                    double xj = (type[j] == 1) ? x[j] : 0.0;
+                    acc += w * (xi - xj);
+                }
+                y[i] = acc;
+            }
+}
+
+/* FP64 Jacobi-preconditioned CG on the kappa operator from x (in/out).
+ * Returns iterations used; *relres = ||s - A x|| / ||s|| (solid rows). */
+int o_kappa_pcg64(int lx, int ly, int lz, const double *kappa, const uint8_t *type, const double *s, double *x,
+                  double tol, int maxit, double *relres) {
+    int64_t n = (int64_t)lx * ly * lz;
+    double *r = malloc(n * 8), *z = malloc(n * 8), *p = malloc(n * 8), *q = malloc(n * 8), *dinv = malloc(n * 8);
+    for (int zz = 0; zz < lz; zz++)
+        for (int yy = 0; yy < ly; yy++)
+            for (int xx = 0; xx < lx; xx++) {
+                int64_t i = gidx(xx, yy, zz, lx, ly);
+                double d = 0.0;
+                if (type[i] == 1)
+                    for (int k = 0; k < 26; k++) {
+                        int nx = xx + OFS[k][0], ny = yy + OFS[k][1], nz = zz + OFS[k][2];
+                        if (!inb(nx, ny, nz, lx, ly, lz)) continue;
+                        int64_t j = gidx(nx, ny, nz, lx, ly);
+                        if (type[j] == 0) continue;
+                        d += KC[k] * hm(kappa[i], kappa[j]);
+                    }
+                dinv[i] = d > 0.0 ? 1.0 / d : 0.0;
+                if (type[i] != 1) x[i] = 0.0;
+            }
+    o_kappa_apply(lx, ly, lz, kappa, type, x, q);
+    double bn = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        double si = type[i] == 1 ? s[i] : 0.0;
+        r[i] = si - q[i];
+        bn += si * si;
+    }
+    bn = sqrt(bn);
+    if (bn == 0.0) bn = 1.0;
+    double rz = 0.0;
+    for (int64_t i = 0; i < n; i++) { z[i] = dinv[i] * r[i]; p[i] = z[i]; rz += r[i] * z[i]; }
+    int it = 0;
+    double rn = 0.0;
+    for (it = 0; it < maxit; it++) {
+        rn = 0.0;
+        for (int64_t i = 0; i < n; i++) rn += r[i] * r[i];
+        rn = sqrt(rn) / bn;
+        if (rn <= tol) break;
+        o_kappa_apply(lx, ly, lz, kappa, type, p, q);
+        double pq = 0.0;
+        for (int64_t i = 0; i < n; i++) pq += p[i] * q[i];
+        if (pq == 0.0) break;
+        double a = rz / pq, rz2 = 0.0;
+        for (int64_t i = 0; i < n; i++) { x[i] += a * p[i]; r[i] -= a * q[i]; z[i] = dinv[i] * r[i]; rz2 += r[i] * z[i]; }
+        double b = rz2 / rz;
+        rz = rz2;
+        for (int64_t i = 0; i < n; i++) p[i] = z[i] + b * p[i];
+    }
+    /* true residual */
+    o_kappa_apply(lx, ly, lz, kappa, type, x, q);
+    rn = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        if (type[i] != 1) continue;
+        double d = s[i] - q[i];
+        rn += d * d;
+    }
+    *relres = sqrt(rn) / bn;
+    free(r); free(z); free(p); free(q); free(dinv);
+    return it;
+}
+
+/* relative residual of an FP32 solution against the FP64 operator */
+double o_kappa_relres(int lx, int ly, int lz, const double *kappa, const uint8_t *type, const double *s,
+                      const float *phi32) {
+    int64_t n = (int64_t)lx * ly * lz;
+    double *x = malloc(n * 8), *q = malloc(n * 8);
+    for (int64_t i = 0; i < n; i++) x[i] = type[i] == 1 ? (double)phi32[i] : 0.0;
+    o_kappa_apply(lx, ly, lz, kappa, type, x, q);
+    double rn = 0.0, bn = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        if (type[i] != 1) continue;
+        double d = s[i] - q[i];
+        rn += d * d;
+        bn += s[i] * s[i];
+    }
+    free(x); free(q);
+    return bn > 0.0 ? sqrt(rn / bn) : sqrt(rn);
+}

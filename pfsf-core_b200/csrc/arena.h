@@ -1,0 +1,23 @@
+// Packed device arena of the tolerance solve (one allocation per island set).
+#pragma once
+#include <vector>
+
+#include "engine.h"
+#include "kappa.h"
+
+namespace pfsf_b200 {
+
+struct Engine::Arena {
+    std::vector<int32_t> ids;        // island ids in arena order
+    std::vector<KDesc> desc;         // host copy of descriptors
+    int prec = -1;
+    int64_t nfine = 0, ncoarse = 0;
+    void* base = nullptr;            // single device allocation
+    size_t bytes = 0;
+    KArena dev{};                    // device pointers (into base)
+    float* hscratch = nullptr;       // pinned host scalars (plain mode)
+    float* phi_out = nullptr;        // FP32 solution staging (device), aliases e
+    std::vector<void*> pinned;       // host ranges registered for fast copies
+};
+
+}  // namespace pfsf_b200

@@ -1,0 +1,200 @@
+// PFSF B200 engine: island registry, device buffers, per-tick schedule.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "pfsf/pfsf.h"
+
+namespace pfsf_b200 {
+
+// Reference constants (L1-native/libpfsf/src/core/constants.h).
+constexpr int kWarmupSteps = 8;
+constexpr float kDampingFactor = 0.995f;
+constexpr int kMgInterval = 4;
+constexpr int kStepsMajor = 16;
+constexpr int kPcgMinRbgs = 2;
+constexpr int kPcgMinSteps = 1;
+constexpr int64_t kPcgMaxN = 512LL * 512LL;
+constexpr float kPfL0 = 2.0f;  // max(PHASE_FIELD_L0 = 1.5, 2)
+constexpr float kPfGc = 100.0f;
+constexpr float kPfRelax = 0.3f;
+constexpr int kSparseCapacity = 512;
+constexpr int kSparseRecordBytes = 48;
+
+struct HostBuffers {
+    bool registered = false;
+    void* phi = nullptr;
+    int64_t phi_bytes = 0;
+    void* source = nullptr;
+    int64_t source_bytes = 0;
+    void* conductivity = nullptr;
+    int64_t conductivity_bytes = 0;
+    void* voxel_type = nullptr;
+    int64_t voxel_type_bytes = 0;
+    void* rcomp = nullptr;
+    int64_t rcomp_bytes = 0;
+    void* rtens = nullptr;
+    int64_t rtens_bytes = 0;
+    void* max_phi = nullptr;
+    int64_t max_phi_bytes = 0;
+    bool lookups_registered = false;
+    void* curing = nullptr;
+    int64_t curing_bytes = 0;
+    void* stress_out = nullptr;
+    int64_t stress_bytes = 0;
+    // kappa-form inputs (pfsf_register_island_kappa)
+    bool kappa_registered = false;
+    void* k_phi = nullptr;
+    void* k_source = nullptr;
+    void* k_kappa = nullptr;
+    void* k_type = nullptr;
+};
+
+// Small device-side per-island tick result, read back in one copy.
+struct TickResult {
+    float macro_max;
+    int32_t fail_total;
+    int32_t pad[2];
+};
+
+struct KappaState;  // tolerance-solve state (kappa_solver.cu)
+
+struct Island {
+    int32_t id = 0;
+    pfsf_pos origin{0, 0, 0};
+    int lx = 0, ly = 0, lz = 0;
+    int64_t n = 0, nmb = 0;
+    bool dirty = true;
+    HostBuffers hosts;
+
+    // fine level (device)
+    float *phi = nullptr, *src = nullptr, *sigma = nullptr, *rcomp = nullptr, *rtens = nullptr,
+          *maxphi = nullptr, *hyd = nullptr, *H = nullptr, *D = nullptr;
+    uint8_t *type = nullptr, *fail = nullptr;
+    uint32_t* macro = nullptr;
+    TickResult* result = nullptr;
+    int32_t *fcounts = nullptr, *foffsets = nullptr, *tuples = nullptr;
+    int32_t tuple_cap = 0;
+
+    // multigrid (two coarse levels, reference island_buffer.cpp:179-188)
+    bool mg_alloc = false, mg_dirty = true;
+    int l1[3] = {0, 0, 0}, l2[3] = {0, 0, 0};
+    int64_t n1 = 0, n2 = 0;
+    float *phi1[2] = {nullptr, nullptr}, *src1 = nullptr, *sig1 = nullptr;
+    float *phi2[2] = {nullptr, nullptr}, *src2 = nullptr, *sig2 = nullptr;
+    uint8_t *type1 = nullptr, *type2 = nullptr;
+    int cur1 = 0, cur2 = 0;
+
+    // PCG (allocated on the first stalled tick, dispatcher.cpp:133)
+    bool pcg_alloc = false;
+    float *r[2] = {nullptr, nullptr}, *p = nullptr, *ap = nullptr, *invdiag = nullptr, *partial = nullptr,
+          *red = nullptr;
+    int rcur = 0;
+
+    // sparse upload region (pinned host) + device staging
+    void* sparse_host = nullptr;
+    void* sparse_dev = nullptr;
+
+    // schedule state
+    int chebyshev_iter = 0;
+    float prev_macro = 0.0f, last_macro = 0.0f;
+
+    std::unique_ptr<KappaState> kappa;
+
+    std::vector<std::pair<void*, size_t>> allocations;  // device allocations owned by this island
+    std::vector<void*> host_registered;
+    Island();
+    ~Island();
+};
+
+class Engine {
+public:
+    explicit Engine(const pfsf_config& cfg);
+    ~Engine();
+
+    pfsf_result init();
+    void shutdown();
+    bool available() const { return available_; }
+    pfsf_result get_stats(pfsf_stats* out);
+
+    pfsf_result add_island(const pfsf_island_desc* d);
+    void remove_island(int32_t id);
+    pfsf_result notify_block_change(int32_t id, const pfsf_voxel_update* u);
+    void mark_full_rebuild(int32_t id);
+    pfsf_result register_buffers(int32_t id, const pfsf_island_buffers* b);
+    pfsf_result register_lookups(int32_t id, const pfsf_island_lookups* l);
+    pfsf_result register_stress(int32_t id, void* addr, int64_t bytes);
+    pfsf_result tick(const int32_t* ids, int32_t count, pfsf_tick_result* result, void* fail_addr,
+                     int64_t fail_bytes);
+    pfsf_result read_stress(int32_t id, float* out, int32_t cap, int32_t* count);
+    pfsf_result get_sparse_buffer(int32_t id, void** addr, int64_t* bytes);
+    pfsf_result notify_sparse(int32_t id, int32_t count);
+
+    void set_pcg_enabled(bool on) { pcg_enabled_ = on; }
+    void set_wind(const pfsf_vec3* w) { wind_ = w ? *w : pfsf_vec3{0, 0, 0}; }
+    void set_precision(pfsf_precision p) { precision_ = p; }
+    void set_solve_mode(pfsf_solve_mode m) { solve_mode_ = m; }
+
+    pfsf_result register_kappa(int32_t id, const pfsf_island_kappa_buffers* b);
+    pfsf_result solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter, uint32_t flags,
+                                   pfsf_solve_stats* out);
+    pfsf_result read_solution64(int32_t id, double* out, int64_t cap, int64_t* count);
+    pfsf_result debug_read_field(int32_t id, int32_t field, void* out, int64_t bytes, int64_t* out_bytes);
+
+    cudaStream_t stream() const { return stream_; }
+    int64_t launches() const { return launches_.load(); }
+    void count_launches(int64_t k) { launches_ += k; }
+
+    // device allocation with budget accounting and an optional injected failure
+    // (for host-side fault-injection tests: PFSF_FAULT_ALLOC_AFTER=<k> fails
+    // the (k+1)-th allocation).
+    void* dalloc(Island& isl, size_t bytes);
+    Island* find(int32_t id);
+
+private:
+    bool ensure_compat(Island& isl);
+    bool build_arena(const std::vector<Island*>& set);
+    void free_arena();
+    bool upload(Island& isl);
+    bool ensure_mg(Island& isl);
+    bool ensure_pcg(Island& isl);
+    void rbgs_step(Island& isl, float damping);
+    int vcycle(Island& isl);
+    bool try_vcycle(Island& isl, int k, bool mg_available);
+    void coarse_pass(Island& isl, int level, float damping);
+    void pcg_initial(Island& isl);
+    void pcg_step(Island& isl, bool first);
+    int solve_steps(Island& isl, int steps);
+    void free_island(Island& isl);
+
+    pfsf_config cfg_;
+    bool available_ = false;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    std::map<int32_t, std::unique_ptr<Island>> islands_;
+    bool pcg_enabled_ = true;
+    pfsf_vec3 wind_{0, 0, 0};
+    pfsf_precision precision_ = PFSF_PREC_FP32;
+    pfsf_solve_mode solve_mode_ = PFSF_SOLVE_PER_ISLAND;
+    std::atomic<int64_t> launches_{0};
+    int64_t vram_used_ = 0;
+    int64_t alloc_count_ = 0;
+    int64_t fault_alloc_after_ = -1;
+    mutable std::mutex stats_mtx_;
+    float last_tick_ms_ = 0.0f;
+    TickResult* host_results_ = nullptr;  // pinned
+    int host_results_cap_ = 0;
+
+    // tolerance-solve arena (one packed allocation for a set of islands)
+    struct Arena;
+    std::unique_ptr<Arena> arena_;
+    int num_sms_ = 148;
+};
+
+}  // namespace pfsf_b200

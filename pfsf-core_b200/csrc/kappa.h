@@ -1,0 +1,79 @@
+// Tolerance solve of the symmetric harmonic-mean 26-point operator.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfsf_b200 {
+
+constexpr int kMaxLevels = 5;
+
+struct KLevel {
+    int lx, ly, lz;
+    int pad;
+    int64_t off;  // first cell of this level in the coarse arrays
+    int64_t n;    // cells
+};
+
+// Per-island descriptor (device resident).
+struct KDesc {
+    int lx, ly, lz, nlev;
+    int64_t off;  // first voxel in the fine arrays
+    int64_t n;
+    KLevel lev[kMaxLevels];  // lev[0] unused (fine level), 1..nlev-1 coarse
+    // results
+    double relres;
+    double bnorm;
+    int inner_iters, outer_iters, converged, status;
+};
+
+// Device pointers and parameters of one batched solve.
+struct KArena {
+    const uint8_t* type;
+    const float* k32;      // sanitised kappa (0 on air), FP32
+    const uint16_t* k16;   // kappa rounded to BF16 / FP16 (preconditioner)
+    const float* b;        // source (0 off solid voxels)
+    double* x64;           // solution accumulator
+    float *r, *e, *z, *p, *q;
+    float* cdiag;          // coarse diagonal (FP32)
+    uint16_t* coef16;      // coarse off-diagonals, 26 per cell (16-bit)
+    float* coef32;         // coarse off-diagonals, 26 per cell (FP32)
+    float *cx, *cb;        // coarse solution / right-hand side
+    KDesc* desc;
+    const int* order;      // island processing order (largest first)
+    int* queue;            // work counter
+    int nisl;
+    int prec;              // 0 fp32, 1 bf16, 2 fp16 (preconditioner storage)
+    double tol;
+    double eta_min;
+    int max_inner, max_outer;
+    float omega_c;
+    int nu;                // pre/post smoothing sweeps
+    int coarse_sweeps;     // symmetric sweeps on the coarsest level
+    int fp64_dots;         // inner products in FP64 (1) or FP32 (0)
+    float* scratch;        // plain mode: block partials + scalars (device)
+    float* hscratch;       // plain mode: pinned host scalars
+};
+
+struct KappaState {
+    bool registered = false;
+    void* h_phi = nullptr;
+    void* h_src = nullptr;
+    void* h_kappa = nullptr;
+    void* h_type = nullptr;
+};
+
+namespace kappa {
+// Plans levels for an island (host).
+int plan_levels(int lx, int ly, int lz, KLevel* lev);
+// Batched solve: one persistent launch over all islands in arena.
+void launch_batched(cudaStream_t s, const KArena& a, int ctas, int threads);
+// Prepare kernels: sanitise kappa, round to 16-bit, zero non-solid source.
+void launch_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total, const int64_t* dummy);
+// Per-island plain solve driven from the host (one kernel per operation).
+// Returns kernel launches issued; writes results into desc (device) and hres (host copy).
+int64_t solve_plain(cudaStream_t s, const KArena& a, int isl, const KDesc& hdesc, KDesc* hres);
+int batched_threads();
+int64_t plain_scratch_floats();
+}  // namespace kappa
+
+}  // namespace pfsf_b200

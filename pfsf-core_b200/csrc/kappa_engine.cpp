@@ -1,0 +1,273 @@
+// Engine side of the tolerance solve: kappa-form registration, the packed
+// device arena for a set of islands, upload / solve / readback.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "arena.h"
+
+namespace pfsf_b200 {
+
+#define CU_OK(expr) (cudaSuccess == (expr))
+
+namespace kappa {
+void launch_to_f32(cudaStream_t s, const KArena& a, int64_t n);
+}
+
+namespace {
+constexpr int64_t kAlignElems = 32;
+inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+}  // namespace
+
+pfsf_result Engine::register_kappa(int32_t id, const pfsf_island_kappa_buffers* b) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (!b || !b->phi_addr || !b->source_addr || !b->kappa_addr || !b->voxel_type_addr)
+        return PFSF_ERROR_INVALID_ARG;
+    Island* s = find(id);
+    if (!s) return PFSF_ERROR_INVALID_ARG;
+    const int64_t n = s->n;
+    if (b->phi_bytes < 4 * n || b->source_bytes < 4 * n || b->kappa_bytes < 4 * n || b->voxel_type_bytes < n)
+        return PFSF_ERROR_INVALID_ARG;
+    HostBuffers& h = s->hosts;
+    h.k_phi = b->phi_addr;
+    h.k_source = b->source_addr;
+    h.k_kappa = b->kappa_addr;
+    h.k_type = b->voxel_type_addr;
+    h.kappa_registered = true;
+    if (!s->kappa) s->kappa.reset(new KappaState());
+    s->kappa->registered = true;
+    // the arena is rebuilt (and re-uploaded) when its island set changes
+    if (arena_) {
+        auto& ids = arena_->ids;
+        if (std::find(ids.begin(), ids.end(), id) != ids.end()) arena_->prec = -2;  // force re-upload
+    }
+    return PFSF_OK;
+}
+
+void Engine::free_arena() {
+    if (!arena_) return;
+    cudaStreamSynchronize(stream_);
+    for (void* h : arena_->pinned) cudaHostUnregister(h);
+    if (arena_->base) cudaFree(arena_->base);
+    if (arena_->hscratch) cudaFreeHost(arena_->hscratch);
+    {
+        std::lock_guard<std::mutex> lk(stats_mtx_);
+        vram_used_ -= (int64_t)arena_->bytes;
+    }
+    arena_.reset();
+}
+
+bool Engine::build_arena(const std::vector<Island*>& set) {
+    free_arena();
+    auto A = std::make_unique<Arena>();
+    A->prec = (int)precision_;
+    int64_t fine = 0, coarse = 0;
+    for (Island* s : set) {
+        KDesc d{};
+        d.lx = s->lx; d.ly = s->ly; d.lz = s->lz;
+        d.n = s->n;
+        d.off = fine;
+        fine = align_up(fine + s->n, kAlignElems);
+        d.nlev = kappa::plan_levels(s->lx, s->ly, s->lz, d.lev);
+        for (int l = 1; l < d.nlev; l++) {
+            d.lev[l].off = coarse;
+            coarse = align_up(coarse + d.lev[l].n, kAlignElems);
+        }
+        A->desc.push_back(d);
+        A->ids.push_back(s->id);
+    }
+    if (coarse == 0) coarse = kAlignElems;
+    A->nfine = fine;
+    A->ncoarse = coarse;
+    const int nisl = (int)set.size();
+    const size_t cbytes = A->prec > 0 ? 2 : 4;
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off = (off + b + 255) / 256 * 256; return o; };
+    const size_t o_type = take(fine), o_k32 = take(fine * 4), o_k16 = take(fine * 2), o_b = take(fine * 4),
+                 o_x64 = take(fine * 8), o_r = take(fine * 4), o_e = take(fine * 4), o_z = take(fine * 4),
+                 o_p = take(fine * 4), o_q = take(fine * 4), o_cd = take(coarse * 4), o_cf = take(coarse * 26 * cbytes),
+                 o_cx = take(coarse * 4), o_cb = take(coarse * 4), o_desc = take(sizeof(KDesc) * nisl),
+                 o_order = take(sizeof(int) * nisl), o_queue = take(256),
+                 o_scr = take(sizeof(float) * kappa::plain_scratch_floats());
+    A->bytes = off;
+    if (fault_alloc_after_ >= 0 && alloc_count_ >= fault_alloc_after_) return false;
+    if (cudaMalloc(&A->base, A->bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    alloc_count_++;
+    {
+        std::lock_guard<std::mutex> lk(stats_mtx_);
+        vram_used_ += (int64_t)A->bytes;
+    }
+    cudaMemsetAsync(A->base, 0, A->bytes, stream_);
+    char* b = static_cast<char*>(A->base);
+    KArena& k = A->dev;
+    k.type = reinterpret_cast<uint8_t*>(b + o_type);
+    k.k32 = reinterpret_cast<float*>(b + o_k32);
+    k.k16 = reinterpret_cast<uint16_t*>(b + o_k16);
+    k.b = reinterpret_cast<float*>(b + o_b);
+    k.x64 = reinterpret_cast<double*>(b + o_x64);
+    k.r = reinterpret_cast<float*>(b + o_r);
+    k.e = reinterpret_cast<float*>(b + o_e);
+    k.z = reinterpret_cast<float*>(b + o_z);
+    k.p = reinterpret_cast<float*>(b + o_p);
+    k.q = reinterpret_cast<float*>(b + o_q);
+    k.cdiag = reinterpret_cast<float*>(b + o_cd);
+    k.coef16 = reinterpret_cast<uint16_t*>(b + o_cf);
+    k.coef32 = reinterpret_cast<float*>(b + o_cf);
+    k.cx = reinterpret_cast<float*>(b + o_cx);
+    k.cb = reinterpret_cast<float*>(b + o_cb);
+    k.desc = reinterpret_cast<KDesc*>(b + o_desc);
+    k.order = reinterpret_cast<int*>(b + o_order);
+    k.queue = reinterpret_cast<int*>(b + o_queue);
+    k.scratch = reinterpret_cast<float*>(b + o_scr);
+    k.nisl = nisl;
+    k.prec = A->prec;
+    if (!CU_OK(cudaMallocHost((void**)&A->hscratch, 256))) return false;
+    k.hscratch = A->hscratch;
+    // largest island first (load balance of the persistent queue)
+    std::vector<int> order(nisl);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return A->desc[a].n > A->desc[c].n; });
+    cudaMemcpyAsync(const_cast<int*>(k.order), order.data(), sizeof(int) * nisl, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(k.desc, A->desc.data(), sizeof(KDesc) * nisl, cudaMemcpyHostToDevice, stream_);
+    for (Island* s : set) {
+        const HostBuffers& h = s->hosts;
+        const void* ptrs[4] = {h.k_phi, h.k_source, h.k_kappa, h.k_type};
+        const size_t sz[4] = {(size_t)s->n * 4, (size_t)s->n * 4, (size_t)s->n * 4, (size_t)s->n};
+        for (int q = 0; q < 4; q++) {
+            if (cudaHostRegister(const_cast<void*>(ptrs[q]), sz[q], cudaHostRegisterDefault) == cudaSuccess)
+                A->pinned.push_back(const_cast<void*>(ptrs[q]));
+            else
+                cudaGetLastError();
+        }
+    }
+    if (!CU_OK(cudaStreamSynchronize(stream_))) return false;
+    arena_ = std::move(A);
+    return true;
+}
+
+pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
+                                       uint32_t flags, pfsf_solve_stats* out) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (count < 0 || (count > 0 && !ids) || !(tol > 0.0)) return PFSF_ERROR_INVALID_ARG;
+    std::vector<Island*> set;
+    for (int32_t k = 0; k < count; k++) {
+        Island* s = find(ids[k]);
+        if (!s || !s->hosts.kappa_registered) return PFSF_ERROR_INVALID_ARG;
+        if (std::find(set.begin(), set.end(), s) == set.end()) set.push_back(s);
+    }
+    pfsf_solve_stats st{};
+    st.struct_bytes = (int32_t)sizeof(pfsf_solve_stats);
+    if (set.empty()) {
+        if (out) *out = st;
+        return PFSF_OK;
+    }
+    bool same = arena_ && arena_->prec == (int)precision_ && arena_->ids.size() == set.size();
+    if (same)
+        for (size_t k = 0; k < set.size(); k++) same &= arena_->ids[k] == set[k]->id;
+    bool do_upload = !(flags & PFSF_SOLVE_NO_UPLOAD);
+    if (!same) {
+        if (!build_arena(set)) return PFSF_ERROR_OUT_OF_VRAM;
+        do_upload = true;
+    }
+    Arena& A = *arena_;
+    KArena k = A.dev;
+    k.tol = tol;
+    k.eta_min = 1e-4;
+    k.max_outer = 8;
+    k.max_inner = max_iter > 0 ? max_iter : 500;
+    k.omega_c = 1.8f;
+    k.nu = 2;
+    k.coarse_sweeps = 4;
+    const bool batched = solve_mode_ == PFSF_SOLVE_BATCHED;
+    k.fp64_dots = batched ? 1 : 0;
+
+    cudaEvent_t ev[4];
+    for (auto& e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[0], stream_);
+    if (do_upload) {
+        for (size_t q = 0; q < set.size(); q++) {
+            const Island* s = set[q];
+            const KDesc& d = A.desc[q];
+            const size_t n = (size_t)s->n;
+            bool ok = true;
+            ok &= CU_OK(cudaMemcpyAsync(const_cast<uint8_t*>(k.type) + d.off, s->hosts.k_type, n,
+                                        cudaMemcpyHostToDevice, stream_));
+            ok &= CU_OK(cudaMemcpyAsync(const_cast<float*>(k.k32) + d.off, s->hosts.k_kappa, n * 4,
+                                        cudaMemcpyHostToDevice, stream_));
+            ok &= CU_OK(cudaMemcpyAsync(const_cast<float*>(k.b) + d.off, s->hosts.k_source, n * 4,
+                                        cudaMemcpyHostToDevice, stream_));
+            ok &= CU_OK(cudaMemcpyAsync(k.e + d.off, s->hosts.k_phi, n * 4, cudaMemcpyHostToDevice, stream_));
+            if (!ok) return PFSF_ERROR_VULKAN;
+        }
+        kappa::launch_prepare(stream_, k, A.nfine, nullptr);
+        launches_++;
+    }
+    cudaEventRecord(ev[1], stream_);
+    int64_t nl = 0;
+    std::vector<KDesc> res(set.size());
+    if (batched) {
+        cudaMemsetAsync(k.queue, 0, sizeof(int), stream_);
+        int per_sm = 2;
+        const int ctas = std::max(1, std::min((int)set.size(), num_sms_ * per_sm));
+        kappa::launch_batched(stream_, k, ctas, kappa::batched_threads());
+        nl = 1;
+    } else {
+        for (size_t q = 0; q < set.size(); q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &res[q]);
+    }
+    cudaEventRecord(ev[2], stream_);
+    launches_ += nl;
+    if (!(flags & PFSF_SOLVE_NO_READBACK)) {
+        kappa::launch_to_f32(stream_, k, A.nfine);
+        launches_++;
+        nl++;
+        for (size_t q = 0; q < set.size(); q++) {
+            const Island* s = set[q];
+            if (!CU_OK(cudaMemcpyAsync(s->hosts.k_phi, k.e + A.desc[q].off, (size_t)s->n * 4, cudaMemcpyDeviceToHost,
+                                       stream_)))
+                return PFSF_ERROR_VULKAN;
+        }
+    }
+    cudaMemcpyAsync(res.data(), k.desc, sizeof(KDesc) * set.size(), cudaMemcpyDeviceToHost, stream_);
+    cudaEventRecord(ev[3], stream_);
+    if (!CU_OK(cudaStreamSynchronize(stream_))) return PFSF_ERROR_VULKAN;
+    float t_up = 0, t_solve = 0, t_rb = 0;
+    cudaEventElapsedTime(&t_up, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_solve, ev[1], ev[2]);
+    cudaEventElapsedTime(&t_rb, ev[2], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    st.islands_solved = (int32_t)set.size();
+    for (const KDesc& d : res) {
+        st.islands_converged += d.converged ? 1 : 0;
+        st.max_iterations = std::max(st.max_iterations, d.inner_iters);
+        st.max_rel_residual = std::max(st.max_rel_residual, d.relres);
+    }
+    st.device_ms = t_solve;
+    st.upload_ms = t_up;
+    st.readback_ms = t_rb;
+    st.kernel_launches = (int32_t)std::min<int64_t>(nl, INT32_MAX);
+    A.desc = res;
+    if (out) *out = st;
+    return PFSF_OK;
+}
+
+pfsf_result Engine::read_solution64(int32_t id, double* out, int64_t cap, int64_t* count) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (!out || !count) return PFSF_ERROR_INVALID_ARG;
+    *count = 0;
+    if (!arena_) return PFSF_ERROR_INVALID_ARG;
+    auto it = std::find(arena_->ids.begin(), arena_->ids.end(), id);
+    if (it == arena_->ids.end()) return PFSF_ERROR_INVALID_ARG;
+    const KDesc& d = arena_->desc[it - arena_->ids.begin()];
+    const int64_t n = std::min<int64_t>(d.n, cap);
+    if (n <= 0) return PFSF_OK;
+    if (!CU_OK(cudaMemcpyAsync(out, arena_->dev.x64 + d.off, (size_t)n * 8, cudaMemcpyDeviceToHost, stream_)) ||
+        !CU_OK(cudaStreamSynchronize(stream_)))
+        return PFSF_ERROR_VULKAN;
+    *count = n;
+    return PFSF_OK;
+}
+
+}  // namespace pfsf_b200

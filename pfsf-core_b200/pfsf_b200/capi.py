@@ -1,0 +1,263 @@
+"""ctypes binding of libpfsf.so (the C ABI in include/pfsf/*.h).
+
+This is the binding a Python caller -- or a test -- uses; the Java caller
+binds the same symbols through JNI.  Loading fails
+loudly when the library has not been built: there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libpfsf.so")
+
+# ---- pfsf_types.h
+PFSF_OK, PFSF_ERROR_VULKAN, PFSF_ERROR_NO_DEVICE, PFSF_ERROR_OUT_OF_VRAM = 0, -1, -2, -3
+PFSF_ERROR_INVALID_ARG, PFSF_ERROR_NOT_INIT, PFSF_ERROR_ISLAND_FULL = -4, -5, -6
+PREC_FP32, PREC_BF16, PREC_FP16 = 0, 1, 2
+SOLVE_PER_ISLAND, SOLVE_BATCHED = 0, 1
+SOLVE_NO_UPLOAD, SOLVE_NO_READBACK = 0x1, 0x2
+
+
+class Pos(C.Structure):
+    _fields_ = [("x", C.c_int32), ("y", C.c_int32), ("z", C.c_int32)]
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class IslandDesc(C.Structure):
+    _fields_ = [("island_id", C.c_int32), ("origin", Pos), ("lx", C.c_int32), ("ly", C.c_int32),
+                ("lz", C.c_int32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("max_island_size", C.c_int32), ("tick_budget_ms", C.c_int32),
+                ("vram_budget_bytes", C.c_int64), ("enable_phase_field", C.c_bool),
+                ("enable_multigrid", C.c_bool)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("island_count", C.c_int32), ("total_voxels", C.c_int64), ("vram_used_bytes", C.c_int64),
+                ("vram_budget_bytes", C.c_int64), ("last_tick_ms", C.c_float)]
+
+
+class FailureEvent(C.Structure):
+    _fields_ = [("pos", Pos), ("type", C.c_int32)]
+
+
+class TickResult(C.Structure):
+    _fields_ = [("events", C.POINTER(FailureEvent)), ("capacity", C.c_int32), ("count", C.c_int32)]
+
+
+class VoxelUpdate(C.Structure):
+    _fields_ = [("flat_index", C.c_int32), ("source", C.c_float), ("type", C.c_int32), ("max_phi", C.c_float),
+                ("rcomp", C.c_float), ("cond", C.c_float * 6)]
+
+
+class IslandBuffers(C.Structure):
+    _fields_ = [(n, t) for pair in [("phi", None), ("source", None), ("conductivity", None), ("voxel_type", None),
+                                    ("rcomp", None), ("rtens", None), ("max_phi", None)]
+                for n, t in ((pair[0] + "_addr", C.c_void_p), (pair[0] + "_bytes", C.c_int64))]
+
+
+class IslandLookups(C.Structure):
+    _fields_ = [(n, t) for pair in ["material_id", "anchor_bitmap", "fluid_pressure", "curing"]
+                for n, t in ((pair + "_addr", C.c_void_p), (pair + "_bytes", C.c_int64))]
+
+
+class KappaBuffers(C.Structure):
+    _fields_ = [(n, t) for pair in ["phi", "source", "kappa", "voxel_type"]
+                for n, t in ((pair + "_addr", C.c_void_p), (pair + "_bytes", C.c_int64))]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("struct_bytes", C.c_int32), ("islands_solved", C.c_int32), ("islands_converged", C.c_int32),
+                ("max_iterations", C.c_int32), ("max_rel_residual", C.c_double), ("device_ms", C.c_float),
+                ("upload_ms", C.c_float), ("readback_ms", C.c_float), ("kernel_launches", C.c_int32)]
+
+
+_lib = None
+
+
+def load():
+    """Load libpfsf.so; raises if it is missing (build it with pfsf-core_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libpfsf.so not built at {LIB_PATH}; run pfsf-core_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    E = C.c_void_p
+    sig = {
+        "pfsf_create": ([C.POINTER(Config)], E),
+        "pfsf_create_with_vulkan": ([C.POINTER(Config), C.c_void_p], E),
+        "pfsf_init": ([E], C.c_int),
+        "pfsf_shutdown": ([E], None),
+        "pfsf_destroy": ([E], None),
+        "pfsf_is_available": ([E], C.c_bool),
+        "pfsf_get_stats": ([E, C.POINTER(Stats)], C.c_int),
+        "pfsf_set_pcg_enabled": ([E, C.c_int], None),
+        "pfsf_set_wind": ([E, C.POINTER(Vec3)], None),
+        "pfsf_add_island": ([E, C.POINTER(IslandDesc)], C.c_int),
+        "pfsf_remove_island": ([E, C.c_int32], None),
+        "pfsf_notify_block_change": ([E, C.c_int32, C.POINTER(VoxelUpdate)], C.c_int),
+        "pfsf_mark_full_rebuild": ([E, C.c_int32], None),
+        "pfsf_tick": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_int64, C.POINTER(TickResult)], C.c_int),
+        "pfsf_read_stress": ([E, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+        "pfsf_register_island_buffers": ([E, C.c_int32, C.POINTER(IslandBuffers)], C.c_int),
+        "pfsf_register_island_lookups": ([E, C.c_int32, C.POINTER(IslandLookups)], C.c_int),
+        "pfsf_register_stress_readback": ([E, C.c_int32, C.c_void_p, C.c_int64], C.c_int),
+        "pfsf_tick_dbb": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_int64, C.c_void_p, C.c_int64], C.c_int),
+        "pfsf_drain_callbacks": ([E, C.c_void_p, C.c_int32], C.c_int32),
+        "pfsf_get_sparse_upload_buffer": ([E, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_notify_sparse_updates": ([E, C.c_int32, C.c_int32], C.c_int),
+        "pfsf_version": ([], C.c_char_p),
+        "pfsf_register_island_kappa": ([E, C.c_int32, C.POINTER(KappaBuffers)], C.c_int),
+        "pfsf_set_precision_mode": ([E, C.c_int], None),
+        "pfsf_set_solve_mode": ([E, C.c_int], None),
+        "pfsf_solve_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
+                                     C.POINTER(SolveStats)], C.c_int),
+        "pfsf_read_solution64": ([E, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_debug_read_field": ([E, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_get_stream": ([E], C.c_void_p),
+        "pfsf_kernel_launch_count": ([E], C.c_int64),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def default_config(max_island_size=50000, tick_budget_ms=8, vram=512 << 20, phase_field=True, multigrid=True):
+    return Config(max_island_size, tick_budget_ms, vram, phase_field, multigrid)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Engine:
+    """Thin owner of a pfsf_engine handle (mirrors NativePFSFBridge's calls)."""
+
+    def __init__(self, config: Config | None = None):
+        self.L = load()
+        self.h = self.L.pfsf_create(C.byref(config) if config is not None else None)
+        if not self.h:
+            raise RuntimeError("pfsf_create failed")
+        self._keep = {}
+
+    def init(self):
+        return self.L.pfsf_init(self.h)
+
+    def close(self):
+        if self.h:
+            self.L.pfsf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_island(self, iid, dims, origin=(0, 0, 0)):
+        d = IslandDesc(iid, Pos(*origin), *dims)
+        return self.L.pfsf_add_island(self.h, C.byref(d))
+
+    def register_buffers(self, iid, phi, source, cond, vtype, rcomp, rtens, max_phi):
+        arrs = [phi, source, cond, vtype, rcomp, rtens, max_phi]
+        b = IslandBuffers(*[v for a in arrs for v in (_ptr(a), a.nbytes)])
+        self._keep[("buf", iid)] = arrs
+        return self.L.pfsf_register_island_buffers(self.h, iid, C.byref(b))
+
+    def register_lookups(self, iid, material, anchor_bitmap, fluid, curing):
+        arrs = [material, anchor_bitmap, fluid, curing]
+        b = IslandLookups(*[v for a in arrs for v in (_ptr(a), a.nbytes)])
+        self._keep[("lk", iid)] = arrs
+        return self.L.pfsf_register_island_lookups(self.h, iid, C.byref(b))
+
+    def register_stress(self, iid, out):
+        self._keep[("st", iid)] = out
+        return self.L.pfsf_register_stress_readback(self.h, iid, _ptr(out), out.nbytes)
+
+    def tick_dbb(self, ids, failure_buf=None, epoch=0):
+        ids = np.ascontiguousarray(ids, np.int32)
+        if failure_buf is None:
+            return self.L.pfsf_tick_dbb(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, epoch, None, 0)
+        return self.L.pfsf_tick_dbb(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, epoch,
+                                    _ptr(failure_buf), failure_buf.nbytes)
+
+    def register_kappa(self, iid, phi, source, kappa, vtype):
+        arrs = [phi, source, kappa, vtype]
+        b = KappaBuffers(*[v for a in arrs for v in (_ptr(a), a.nbytes)])
+        self._keep[("k", iid)] = arrs
+        return self.L.pfsf_register_island_kappa(self.h, iid, C.byref(b))
+
+    def solve(self, ids, tol=1e-6, max_iter=500, flags=0):
+        ids = np.ascontiguousarray(ids, np.int32)
+        st = SolveStats()
+        rc = self.L.pfsf_solve_to_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, tol,
+                                            max_iter, flags, C.byref(st))
+        return rc, st
+
+    def read_solution64(self, iid, n):
+        out = np.zeros(n, np.float64)
+        cnt = C.c_int64(0)
+        rc = self.L.pfsf_read_solution64(self.h, iid, _ptr(out), n, C.byref(cnt))
+        return rc, out[:cnt.value]
+
+    def read_stress(self, iid, n):
+        out = np.zeros(n, np.float32)
+        cnt = C.c_int32(0)
+        rc = self.L.pfsf_read_stress(self.h, iid, _ptr(out), n, C.byref(cnt))
+        return rc, out[:cnt.value]
+
+    FIELD_DTYPES = {0: np.float32, 1: np.float32, 2: np.float32, 3: np.uint8, 4: np.uint32}
+
+    def debug_field(self, iid, field):
+        """Tick-state array of an island (0 phi, 1 H, 2 d, 3 fail, 4 macro bits) or
+        the schedule state dict (field 5)."""
+        size = C.c_int64(0)
+        tmp = np.zeros(32, np.uint8)
+        rc = self.L.pfsf_debug_read_field(self.h, iid, field, _ptr(tmp), 0, C.byref(size))
+        if rc != PFSF_OK:
+            raise RuntimeError(f"pfsf_debug_read_field rc={rc}")
+        if field == 5:
+            rc = self.L.pfsf_debug_read_field(self.h, iid, field, _ptr(tmp), 20, C.byref(size))
+            iv = tmp[:12].view(np.int32)
+            fv = tmp[12:20].view(np.float32)
+            return {"chebyshev_iter": int(iv[0]), "pcg_allocated": int(iv[1]), "mg_allocated": int(iv[2]),
+                    "prev_macro": float(fv[0]), "last_macro": float(fv[1])}
+        dt = self.FIELD_DTYPES[field]
+        out = np.zeros(size.value // np.dtype(dt).itemsize, dt)
+        rc = self.L.pfsf_debug_read_field(self.h, iid, field, _ptr(out), out.nbytes, C.byref(size))
+        if rc != PFSF_OK:
+            raise RuntimeError(f"pfsf_debug_read_field rc={rc}")
+        return out
+
+    def stats(self):
+        s = Stats()
+        rc = self.L.pfsf_get_stats(self.h, C.byref(s))
+        return rc, s
+
+    def set_precision(self, p):
+        self.L.pfsf_set_precision_mode(self.h, p)
+
+    def set_solve_mode(self, m):
+        self.L.pfsf_set_solve_mode(self.h, m)
+
+    def set_pcg_enabled(self, on):
+        self.L.pfsf_set_pcg_enabled(self.h, int(bool(on)))
+
+    def stream(self):
+        return self.L.pfsf_get_stream(self.h)
+
+    def launches(self):
+        return self.L.pfsf_kernel_launch_count(self.h)

@@ -1,0 +1,202 @@
+"""GPU parity of the reference-schedule tick (pfsf_tick_dbb) against the CPU oracle.
+
+Every case drives libpfsf.so through its C ABI exactly as the Java bridge
+does (pfsf_create -> pfsf_init -> pfsf_add_island ->
+pfsf_register_island_buffers -> pfsf_register_stress_readback aliased to the
+phi buffer -> pfsf_tick_dbb with a failure buffer) and compares with the
+oracle island after every tick.
+
+Tolerances (FP32 path): phi agrees within 1e-5 of max|phi| per tick; the
+failure DBB (count and every {x,y,z,type} tuple) is bit-exact; H and the
+damage field agree within 1e-5 relative to their maxima.
+"""
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+from pfsf_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+PHI_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def eng(lib_built):
+    cfg = capi.default_config(max_island_size=1 << 26, tick_budget_ms=1 << 30)
+    e = capi.Engine(cfg)
+    assert e.init() == capi.PFSF_OK, "CUDA device required"
+    yield e
+    e.close()
+
+
+_next_id = [100]
+
+
+def _setup(eng, case, origin=(3, -2, 7)):
+    iid = _next_id[0]
+    _next_id[0] += 1
+    assert eng.add_island(iid, case["dims"], origin) == capi.PFSF_OK
+    host = {k: np.ascontiguousarray(case[k]).copy() for k in
+            ("phi", "source", "conductivity", "type", "rcomp", "rtens", "max_phi")}
+    assert eng.register_buffers(iid, host["phi"], host["source"], host["conductivity"], host["type"],
+                                host["rcomp"], host["rtens"], host["max_phi"]) == capi.PFSF_OK
+    assert eng.register_stress(iid, host["phi"]) == capi.PFSF_OK  # warm start, as the Java runtime does
+    ref = O.Island(*case["dims"])
+    ref.load(phi=case["phi"], source=case["source"], conductivity=case["conductivity"], type=case["type"],
+             rcomp=case["rcomp"], rtens=case["rtens"], max_phi=case["max_phi"], hydration=case["hydration"])
+    return iid, host, ref
+
+
+def _tick_both(eng, iid, host, ref, origin, cap=4096):
+    fb = np.zeros(1 + 4 * cap, np.int32)
+    fb[0] = 77  # pre-zeroed by pfsf_tick_dbb
+    assert eng.tick_dbb([iid], fb) == capi.PFSF_OK
+    ref.tick()
+    want = ref.failures(origin, capacity=cap)
+    return fb, want
+
+
+def _assert_tick_parity(eng, iid, host, ref, fb, want, t):
+    phi_ref = ref.view("phi")
+    scale = max(float(np.abs(phi_ref).max()), 1e-30)
+    err = float(np.abs(host["phi"].astype(np.float64) - phi_ref).max()) / scale
+    assert err <= PHI_TOL, f"tick {t}: phi rel err {err:.3e}"
+    assert np.array_equal(eng.debug_field(iid, 3), ref.view("fail").astype(np.uint8)), f"tick {t}: fail flags"
+    assert fb[0] == want[0], f"tick {t}: failure count {fb[0]} vs {want[0]}"
+    assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]]), f"tick {t}: failure tuples"
+    for field, name in ((1, "H"), (2, "D")):
+        g = eng.debug_field(iid, field)
+        r = ref.view(name)
+        sc = max(float(np.abs(r).max()), 1e-30)
+        assert float(np.abs(g - r).max()) / sc <= PHI_TOL, f"tick {t}: {name}"
+    st = eng.debug_field(iid, 5)
+    rs = ref.state()
+    assert st["chebyshev_iter"] == rs["chebyshev_iter"]
+    assert st["pcg_allocated"] == rs["pcg_allocated"]
+    assert st["mg_allocated"] == rs["mg_allocated"]
+
+
+@pytest.mark.parametrize("name,ticks", [("block8", 4), ("noise20", 4), ("slab", 3), ("rod", 3), ("tiny", 3)])
+def test_tick_parity(eng, name, ticks):
+    case = cases.compat_case(name)
+    origin = (3, -2, 7)
+    iid, host, ref = _setup(eng, case, origin)
+    for t in range(ticks):
+        eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+        fb, want = _tick_both(eng, iid, host, ref, origin)
+        _assert_tick_parity(eng, iid, host, ref, fb, want, t)
+
+
+def test_pcg_tail_engages_and_matches(eng):
+    """Run until the stall ratio switches the schedule to RBGS(2) + PCG(14)
+    (dispatcher.cpp:123-167) and keep comparing."""
+    case = cases.compat_case("block16")
+    origin = (0, 0, 0)
+    iid, host, ref = _setup(eng, case, origin)
+    saw_pcg = False
+    for t in range(8):
+        eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+        fb, want = _tick_both(eng, iid, host, ref, origin)
+        _assert_tick_parity(eng, iid, host, ref, fb, want, t)
+        saw_pcg |= ref.state()["pcg_allocated"] == 1
+    assert saw_pcg
+
+
+def test_isolated_voxel_no_support_gpu(eng):
+    case, centre = cases.isolated_voxel_case()
+    iid, host, ref = _setup(eng, case, (0, 0, 0))
+    fb, want = _tick_both(eng, iid, host, ref, (0, 0, 0))
+    assert host["phi"][centre] == 0.0
+    assert fb[0] == 1 and fb[4] == 3
+
+
+def test_source_free_gpu(eng):
+    case = cases.compat_case("noise20")
+    case["source"][:] = 0.0
+    iid, host, ref = _setup(eng, case)
+    for _ in range(2):
+        eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+        eng.tick_dbb([iid])
+    assert np.all(host["phi"] == 0.0)
+
+
+def test_failure_buffer_saturation(eng):
+    """More failures than tuples: count saturates at capacity, tuples in voxel order."""
+    case = cases.compat_case("noise20")
+    case["rcomp"][:] = 1e-9
+    case["rtens"][:] = 1e-9
+    origin = (1, 2, 3)
+    iid, host, ref = _setup(eng, case, origin)
+    fb, want = _tick_both(eng, iid, host, ref, origin, cap=5)
+    assert fb[0] == 5
+    assert np.array_equal(fb, want)
+
+
+def test_multi_island_tick_order(eng):
+    """Two dirty islands in one tick: failures appended island by island."""
+    c1 = cases.compat_case("block8")
+    c2 = cases.compat_case("tiny")
+    c1["rcomp"][:] = 1e-9
+    c2["rcomp"][:] = 1e-9
+    o1, o2 = (0, 0, 0), (100, 0, 0)
+    i1, h1, r1 = _setup(eng, c1, o1)
+    i2, h2, r2 = _setup(eng, c2, o2)
+    cap = 4096
+    fb = np.zeros(1 + 4 * cap, np.int32)
+    assert eng.tick_dbb([i1, i2], fb) == capi.PFSF_OK
+    r1.tick()
+    r2.tick()
+    want = np.zeros(1 + 4 * cap, np.int32)
+    r1.failures(o1, capacity=cap, dbb=want)
+    r2.failures(o2, capacity=cap, dbb=want)
+    assert fb[0] == want[0] and fb[0] > 0
+    assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]])
+
+
+def test_reference_fixtures_parity(eng):
+    """The reference's own fixture shapes (inputs only), one tick each."""
+    import glob
+    import os
+    fx = os.path.join(os.path.dirname(__file__), "golden", "fixtures_compat.npz")
+    data = np.load(fx, allow_pickle=False)
+    names = sorted({k.split("__")[0] for k in data.files})
+    assert len(names) >= 10
+    for nm in names:
+        case = {k.split("__")[1]: data[k] for k in data.files if k.startswith(nm + "__")}
+        case["dims"] = tuple(int(v) for v in case["dims"])
+        iid, host, ref = _setup(eng, case, (0, 0, 0))
+        for t in range(2):
+            eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+            fb, want = _tick_both(eng, iid, host, ref, (0, 0, 0))
+            _assert_tick_parity(eng, iid, host, ref, fb, want, t)
+
+
+def test_not_dirty_island_is_skipped(eng):
+    case = cases.compat_case("block8")
+    iid, host, ref = _setup(eng, case)
+    assert eng.tick_dbb([iid]) == capi.PFSF_OK  # first tick (dirty after registration)
+    before = host["phi"].copy()
+    fb = np.zeros(1 + 4 * 16, np.int32)
+    fb[0] = 9
+    assert eng.tick_dbb([iid], fb) == capi.PFSF_OK  # clean: nothing dispatched
+    assert fb[0] == 0
+    assert np.array_equal(before, host["phi"])
+
+
+def test_sparse_scatter_updates_device_arrays(eng):
+    case = cases.compat_case("block8")
+    iid, host, ref = _setup(eng, case)
+    import ctypes as C
+    addr = C.c_void_p()
+    nbytes = C.c_int64()
+    assert eng.L.pfsf_get_sparse_upload_buffer(eng.h, iid, C.byref(addr), C.byref(nbytes)) == capi.PFSF_OK
+    assert nbytes.value == 512 * 48
+    rec = np.frombuffer((C.c_byte * nbytes.value).from_address(addr.value), dtype=np.uint32)
+    rec[:12] = 0
+    rec[0] = 5
+    rec[1:2] = np.array([0.25], np.float32).view(np.uint32)
+    rec[2] = 1
+    assert eng.L.pfsf_notify_sparse_updates(eng.h, iid, 1) == capi.PFSF_OK
+    assert eng.L.pfsf_notify_sparse_updates(eng.h, iid, 0) == capi.PFSF_OK
