@@ -536,24 +536,28 @@ double o_dot(int64_t n, const float *a, const float *b) {
     return acc;
 }
 
-/* ---- phase_field_evolve.comp.glsl:246-364 ---- */
+/* ---- phase_field_evolve.comp.glsl:246-364.  The shader updates dField in
+ * place while neighbouring invocations read it (a race); restated as reading
+ * every d_j from the field as it was before the pass. ---- */
 void o_phase_field(int lx, int ly, int lz, const float *phi, const float *H, float *D, const float *sigma,
                    const uint8_t *type, uint32_t *fail, const float *hyd, float l0, float gc, float relax,
                    int split) {
     int64_t N = (int64_t)lx * ly * lz;
+    float *Dold = (float *)malloc((size_t)N * 4);
+    memcpy(Dold, D, (size_t)N * 4);
     for (int z = 0; z < lz; z++)
         for (int y = 0; y < ly; y++)
             for (int x = 0; x < lx; x++) {
                 int64_t i = gidx(x, y, z, lx, ly);
                 if (type[i] == 0 || type[i] == 2) continue;
                 if (fail[i] != 0) continue;
-                float phi_i = phi[i], sumSigma = 0.0f, lap_phi = 0.0f, lap_d = 0.0f, d_i = D[i];
+                float phi_i = phi[i], sumSigma = 0.0f, lap_phi = 0.0f, lap_d = 0.0f, d_i = Dold[i];
                 for (int d = 0; d < 6; d++) {
                     int nx = x + OFS[d][0], ny = y + OFS[d][1], nz = z + OFS[d][2];
                     if (!inb(nx, ny, nz, lx, ly, lz)) continue;
                     int64_t j = gidx(nx, ny, nz, lx, ly);
                     if (type[j] == 0) continue;
-                    float s = sigma[(int64_t)d * N + i], pj = phi[j], dj = D[j];
+                    float s = sigma[(int64_t)d * N + i], pj = phi[j], dj = Dold[j];
                     if (finitef_(pj)) { lap_phi += (pj - phi_i); sumSigma += s; }
                     if (finitef_(dj)) lap_d += (dj - d_i);
                 }
@@ -577,6 +581,7 @@ void o_phase_field(int lx, int ly, int lz, const float *phi, const float *H, flo
                 D[i] = dn;
                 if (dn > 0.95f) fail[i] = 1;
             }
+    free(Dold);
 }
 
 /* ---- failure_scan.comp.glsl:36-196 ---- */

@@ -559,9 +559,12 @@ __global__ void __launch_bounds__(kBlock) k_finalize(const float* __restrict__ p
 }
 
 // ---------------------------------------------------------------- phase field
-// SH/phase_field_evolve.comp.glsl:246-364
+// SH/phase_field_evolve.comp.glsl:246-364.  The shader rewrites dField in place
+// while neighbours read it (a race); here every d_j comes from Dold, a copy of
+// the field taken before the pass.
 __global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, const float* __restrict__ phi,
                                                         const float* __restrict__ H, float* __restrict__ D,
+                                                        const float* __restrict__ Dold,
                                                         const float* __restrict__ sigma,
                                                         const uint8_t* __restrict__ type,
                                                         uint8_t* __restrict__ fail, const float* __restrict__ hyd,
@@ -575,7 +578,7 @@ __global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, 
     const int x = (int)(i % lx);
     const int64_t rem = i / lx;
     const int y = (int)(rem % ly), z = (int)(rem / ly);
-    const float phi_i = phi[i], d_i = D[i];
+    const float phi_i = phi[i], d_i = Dold[i];
     float sum_sigma = 0.0f, lap_phi = 0.0f, lap_d = 0.0f;
 #pragma unroll
     for (int d = 0; d < 6; d++) {
@@ -583,7 +586,7 @@ __global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, 
         if (!inb(nx, ny, nz, lx, ly, lz)) continue;
         const int64_t j = gidx(nx, ny, nz, lx, ly);
         if (type[j] == kAir) continue;
-        const float s = sigma[d * n + i], pj = phi[j], dj = D[j];
+        const float s = sigma[d * n + i], pj = phi[j], dj = Dold[j];
         if (finite_f(pj)) { lap_phi += (pj - phi_i); sum_sigma += s; }
         if (finite_f(dj)) lap_d += (dj - d_i);
     }
@@ -863,10 +866,10 @@ void finalize(cudaStream_t s, const float* partial, int64_t count, float* red, i
     k_finalize<<<1, kBlock, 0, s>>>(partial, count, red, slot, rotate);
 }
 void phase_field(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* H, float* D,
-                 const float* sigma, const uint8_t* type, uint8_t* fail, const float* hyd, float l0, float gc,
-                 float relax, int split) {
-    k_phase_field<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, H, D, sigma, type, fail, hyd,
-                                                                     l0, gc, relax, split);
+                 const float* Dold, const float* sigma, const uint8_t* type, uint8_t* fail, const float* hyd,
+                 float l0, float gc, float relax, int split) {
+    k_phase_field<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, H, D, Dold, sigma, type, fail,
+                                                                     hyd, l0, gc, relax, split);
 }
 void failure_scan(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const float* rcomp,
                   const uint8_t* type, uint8_t* fail, const float* rtens, uint32_t* macro, const float* rho) {

@@ -179,7 +179,7 @@ bool Engine::ensure_compat(Island& s) {
     bool ok = true;
     auto F = [&](int64_t cnt) { void* p = dalloc(s, (size_t)cnt * 4); ok &= p != nullptr; return (float*)p; };
     s.phi = F(n); s.src = F(n); s.sigma = F(6 * n); s.rcomp = F(n); s.rtens = F(n); s.maxphi = F(n);
-    s.hyd = F(n); s.H = F(n); s.D = F(n);
+    s.hyd = F(n); s.H = F(n); s.D = F(n); s.Dold = F(n);
     s.type = (uint8_t*)dalloc(s, (size_t)n); ok &= s.type != nullptr;
     s.fail = (uint8_t*)dalloc(s, (size_t)n); ok &= s.fail != nullptr;
     s.macro = (uint32_t*)dalloc(s, (size_t)std::max<int64_t>(s.nmb, 1) * 4); ok &= s.macro != nullptr;
@@ -510,8 +510,9 @@ pfsf_result Engine::tick(const int32_t* ids, int32_t count, pfsf_tick_result* re
         launches_++;
         solve_steps(*s, kStepsMajor);
         if (cfg_.enable_phase_field) {
-            compat::phase_field(stream_, s->lx, s->ly, s->lz, s->phi, s->H, s->D, s->sigma, s->type, s->fail, s->hyd,
-                                kPfL0, kPfGc, kPfRelax, 1);
+            cudaMemcpyAsync(s->Dold, s->D, (size_t)s->n * 4, cudaMemcpyDeviceToDevice, stream_);
+            compat::phase_field(stream_, s->lx, s->ly, s->lz, s->phi, s->H, s->D, s->Dold, s->sigma, s->type, s->fail,
+                                s->hyd, kPfL0, kPfGc, kPfRelax, 1);
             launches_++;
         }
         compat::failure_scan(stream_, s->lx, s->ly, s->lz, s->phi, s->sigma, s->rcomp, s->type, s->fail, s->rtens,

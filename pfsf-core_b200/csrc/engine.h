@@ -75,7 +75,7 @@ struct Island {
 
     // fine level (device)
     float *phi = nullptr, *src = nullptr, *sigma = nullptr, *rcomp = nullptr, *rtens = nullptr,
-          *maxphi = nullptr, *hyd = nullptr, *H = nullptr, *D = nullptr;
+          *maxphi = nullptr, *hyd = nullptr, *H = nullptr, *D = nullptr, *Dold = nullptr;
     uint8_t *type = nullptr, *fail = nullptr;
     uint32_t* macro = nullptr;
     TickResult* result = nullptr;
