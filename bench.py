@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark: ms per tick to a 1e-6 relative residual, batched mixed precision
+vs plain FP32 per-island kernels, on one B200 (or N, one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default "batch"): 4096 seeded islands, per-axis log-uniform sides
+scaled to ~6e7 active voxels, value-noise occupancy 60 % kept to the anchored
+26-connected component, three-material mix, point loads on 0.1 % of the top
+surface (pfsf_b200.synth).  A tick solves every island from phi = 0 to
+||s - A phi||_2 / ||s||_2 <= 1e-6 (FP64-evaluated) through the libpfsf C ABI:
+one persistent launch, BF16 kappa / coarse operators in the preconditioner,
+FP32 inner PCG, FP64 inner products and outer residual.
+
+value     device ms per tick with inputs resident in HBM (CUDA events on the
+          engine stream; the arena is far larger than L2, so nothing is cached
+          between steps).
+e2e       the same tick through pfsf_solve_to_tolerance with host buffers:
+          H2D of kappa, source, type and phi0 from pinned memory, D2H of phi.
+plain     the same islands solved one at a time with plain FP32 kernels
+          (one grid-wide launch per operation), timed on a size-stratified
+          sample and scaled by island count.
+Multi-GPU: islands are independent, each rank solves its own workload
+(weak scaling), no collective on the data path; the tick time is the max
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pfsf-core_b200"))
+
+METRIC = "ms/tick to 1e-6 rel. residual: batched mixed-prec vs plain FP32, same B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["batch", "single"], default="batch")
+    ap.add_argument("--islands", type=int, default=4096)
+    ap.add_argument("--target-active", type=float, default=6.0e7)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--precision", choices=["bf16", "fp16", "fp32"], default="bf16")
+    ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_workload(args, rank):
+    from pfsf_b200 import synth
+    if args.workload == "single":
+        isl = synth.noise_island((256, 256, 128), seed=11 + rank)
+        return [isl], {"grid_total": isl.n, "active_total": isl.n_active, "scale": 1.0}
+    return synth.batch(args.islands, seed=7 + 1000 * rank, target_active=args.target_active,
+                       workers=min(32, os.cpu_count() or 1))
+
+
+def stratified(isls, k):
+    """k islands evenly spaced in size order (largest first)."""
+    order = sorted(range(len(isls)), key=lambda i: -isls[i].n)
+    if k >= len(order):
+        return order
+    step = len(order) / k
+    return [order[int(j * step)] for j in range(k)]
+
+
+def cpu_baseline(isls, seconds, tol):
+    """The oracle's FP64 Jacobi-PCG solve (oracle/pfsf_oracle.c o_kappa_pcg64)
+    on a size-stratified sample of islands, one island per host thread,
+    scaled to the whole tick by island count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import concurrent.futures as cf
+    import oracle as O
+
+    O.lib()
+    threads = os.cpu_count() or 1
+    order = sorted(range(len(isls)), key=lambda i: -isls[i].n)
+    # grow the sample (evenly spaced in size order) until the CPU budget is used
+    k = max(threads, 8)
+    t_used = 0.0
+    done = 0
+    while True:
+        sample = stratified(isls, min(k, len(isls)))
+
+        def run(i):
+            s = isls[i]
+            O.kappa_solve64(s.dims, s.kappa.astype(np.float64), s.vtype, s.source.astype(np.float64), tol=tol,
+                            maxit=200000)
+
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(run, sample))
+        t_used = time.perf_counter() - t0
+        done = len(sample)
+        if t_used * 2 > seconds or done >= len(isls):
+            break
+        k = min(len(isls), k * 2)
+    ms = t_used * 1000.0 * len(isls) / done
+    return {"value": ms, "unit": "ms/tick", "cores": threads, "kind": "port",
+            "sample": f"{done} of {len(isls)} islands (size-stratified), FP64 Jacobi-PCG to {tol:g}, "
+                      f"{t_used:.1f} s wall on {threads} threads, scaled by island count"}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.rows = []
+        self.p = None
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                mhz.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_model():
+    """DRAM bytes per active voxel of the batched kernel from the committed ncu
+    summary (profiles/batched_solve_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "batched_solve_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args):
+    ws, rank, _ = dist_info()
+    if rank != 0:
+        return
+    isls, meta = make_workload(args, 0)
+    vals = []
+    cb = None
+    # each step is a bounded, size-stratified sample of the tick (see cpu_baseline)
+    for _ in range(max(args.steps, 1)):
+        cb = cpu_baseline(isls, args.cpu_seconds, args.tol)
+        vals.append(cb["value"])
+    v = float(np.mean(vals))
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "ms/tick", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{len(isls)} islands, {meta['active_total']} active voxels, tol {args.tol:g}",
+                       "islands": len(isls), "active_voxels": meta["active_total"]},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "ms/tick", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    ws, rank, local = dist_info()
+    isls, meta = make_workload(args, rank)  # CPU pool work happens before any CUDA use
+    import torch
+    from pfsf_b200 import capi
+
+    torch.cuda.set_device(local)
+    os.environ["PFSF_CUDA_DEVICE"] = str(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    cfg = capi.default_config(max_island_size=1 << 28, tick_budget_ms=1 << 30, vram=180 << 30)
+    eng = capi.Engine(cfg)
+    rc = eng.init()
+    if rc != capi.PFSF_OK:
+        raise RuntimeError(f"pfsf_init failed rc={rc}")
+    host = []
+    ids = []
+    for k, isl in enumerate(isls):
+        iid = k + 1
+        assert eng.add_island(iid, isl.dims) == capi.PFSF_OK
+        h = {"phi": np.zeros(isl.n, np.float32), "source": isl.source, "kappa": isl.kappa, "type": isl.vtype}
+        assert eng.register_kappa(iid, h["phi"], h["source"], h["kappa"], h["type"]) == capi.PFSF_OK
+        host.append(h)
+        ids.append(iid)
+    prec = {"bf16": capi.PREC_BF16, "fp16": capi.PREC_FP16, "fp32": capi.PREC_FP32}[args.precision]
+    mode = capi.SOLVE_BATCHED if args.workload == "batch" else capi.SOLVE_PER_ISLAND
+    eng.set_solve_mode(mode)
+    eng.set_precision(prec)
+    rc, st0 = eng.solve(ids, tol=args.tol, flags=capi.SOLVE_COLD_START)  # builds and uploads the arena
+    assert rc == capi.PFSF_OK
+    resident = capi.SOLVE_NO_UPLOAD | capi.SOLVE_NO_READBACK | capi.SOLVE_COLD_START
+    for _ in range(args.warmup):
+        eng.solve(ids, tol=args.tol, flags=resident)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = eng.launches()
+    stats = []
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rc, st = eng.solve(ids, tol=args.tol, flags=resident)
+            stats.append(st)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = eng.launches() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    # e2e through the C ABI with host buffers (pinned by the engine at registration)
+    h2d = sum(isl.n * (4 + 4 + 4 + 1) for isl in isls)
+    d2h = sum(isl.n * 4 for isl in isls)
+    e2e = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        rc, st_e = eng.solve(ids, tol=args.tol, flags=capi.SOLVE_COLD_START)
+        e2e.append((time.perf_counter() - t0) * 1000.0)
+    e2e_ms = float(np.mean(e2e))
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    kern_ms = float(np.mean([s.device_ms for s in stats]))
+    conv = min(s.islands_converged for s in stats)
+    maxrel = max(s.max_rel_residual for s in stats)
+    alg_bytes = float(np.mean([s.algorithmic_bytes for s in stats]))
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    tm = traffic_model()
+    traffic = None
+    if tm and tm.get("dram_bytes_per_active_voxel"):
+        traffic = tm["dram_bytes_per_active_voxel"] * st0.active_voxels
+    # FP64-oracle error on a few islands (read the FP64 accumulator back)
+    oracle_err = None
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        errs = []
+        for k in stratified(isls, 4):
+            isl = isls[k]
+            rc, x64 = eng.read_solution64(ids[k], isl.n)
+            xr, _, _ = O.kappa_solve64(isl.dims, isl.kappa.astype(np.float64), isl.vtype,
+                                       isl.source.astype(np.float64), tol=1e-12, maxit=200000)
+            errs.append(float(np.abs(x64 - xr).max() / max(np.abs(xr).max(), 1e-300)))
+        oracle_err = max(errs)
+    # plain FP32 per-island kernels on a stratified sample
+    plain_ms = None
+    plain_note = None
+    if not args.no_plain and args.workload == "batch" and rank == 0:
+        sample = stratified(isls, args.plain_sample)
+        sids = [ids[k] for k in sample]
+        eng.set_solve_mode(capi.SOLVE_PER_ISLAND)
+        eng.set_precision(capi.PREC_FP32)
+        eng.solve(sids, tol=args.tol, flags=capi.SOLVE_COLD_START)
+        rc, stp = eng.solve(sids, tol=args.tol, flags=resident)
+        plain_ms = stp.device_ms * len(isls) / len(sample)
+        plain_note = (f"{len(sample)} of {len(isls)} islands (size-stratified), {stp.device_ms:.1f} ms, "
+                      f"converged {stp.islands_converged}/{len(sample)}, scaled by island count")
+    cb = cpu_baseline(isls, args.cpu_seconds, args.tol) if (rank == 0 and ws == 1) else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms, "unit": "ms/tick", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": (f"{len(isls)} islands/GPU (log-uniform sides, scale {meta['scale']:.3f}), "
+                                    f"{meta['grid_total']} grid / {meta['active_total']} active voxels, "
+                                    f"cold start, tol {args.tol:g}"),
+                       "islands": len(isls), "grid_voxels": meta["grid_total"], "active_voxels": meta["active_total"],
+                       "mode": "batched persistent" if mode == capi.SOLVE_BATCHED else "per-island",
+                       "precision": f"{args.precision} kappa/coarse, fp32 vectors, fp64 dots+outer residual",
+                       "l2": "inputs and solve arena far larger than L2 (126 MB)"},
+            "e2e": {"value": e2e_ms, "unit": "ms/tick", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_batched (persistent solve)", "kernel_ms": kern_ms,
+                         "algorithmic_bytes": alg_bytes},
+            "cpu_baseline": cb,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "converged": f"{conv}/{len(isls)}", "max_rel_residual_fp64": maxrel,
+            "fp64_oracle_error": oracle_err,
+            "plain_fp32_ms_per_tick": plain_ms, "plain_fp32_sample": plain_note,
+            "speedup_vs_plain_fp32": (plain_ms / ms) if plain_ms else None,
+            "inner_iterations_total": int(stats[-1].inner_iterations_total),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -33,6 +33,7 @@ typedef enum {
 /* flags of pfsf_solve_to_tolerance */
 #define PFSF_SOLVE_NO_UPLOAD 0x1u   /* inputs already resident on the device */
 #define PFSF_SOLVE_NO_READBACK 0x2u /* leave phi on the device */
+#define PFSF_SOLVE_COLD_START 0x4u  /* start from phi = 0 instead of the registered phi */
 
 /* Caller-owned host arrays of one island for the tolerance solve. */
 typedef struct pfsf_island_kappa_buffers {
@@ -56,6 +57,10 @@ typedef struct pfsf_solve_stats {
     float upload_ms;
     float readback_ms;
     int32_t kernel_launches; /* kernels launched by the solve */
+    int64_t inner_iterations_total; /* sum over islands of inner PCG iterations */
+    double algorithmic_bytes;       /* compulsory bytes of every pass the solve made:
+                                       each array a pass touches counted once per pass */
+    int64_t active_voxels;          /* solid voxels over all solved islands */
 } pfsf_solve_stats;
 
 /* Registers the kappa-form inputs of an island created by pfsf_add_island.

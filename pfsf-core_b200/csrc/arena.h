@@ -9,6 +9,7 @@ namespace pfsf_b200 {
 
 struct Engine::Arena {
     std::vector<int32_t> ids;        // island ids in arena order
+    std::vector<int64_t> active;     // solid voxels per island
     std::vector<KDesc> desc;         // host copy of descriptors
     int prec = -1;
     int64_t nfine = 0, ncoarse = 0;

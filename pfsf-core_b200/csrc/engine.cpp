@@ -56,6 +56,7 @@ pfsf_result Engine::init() {
     if (dev < 0 || dev >= count) return PFSF_ERROR_NO_DEVICE;
     if (!CU_OK(cudaSetDevice(dev))) return PFSF_ERROR_NO_DEVICE;
     device_ = dev;
+    cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev);
     if (!CU_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) return PFSF_ERROR_VULKAN;
     host_results_cap_ = 256;
     if (!CU_OK(cudaMallocHost((void**)&host_results_, sizeof(TickResult) * host_results_cap_))) {

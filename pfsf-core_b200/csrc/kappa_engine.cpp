@@ -17,6 +17,43 @@ void launch_to_f32(cudaStream_t s, const KArena& a, int64_t n);
 namespace {
 constexpr int64_t kAlignElems = 32;
 inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+// Compulsory bytes of the passes one island's solve made: every array a pass
+// reads or writes counted once per pass (what a perfectly cached streaming
+// implementation must move), per grid voxel / coarse cell.
+double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps) {
+    const double kb = prec > 0 ? 2.0 : 4.0;   // preconditioner kappa
+    const double cb = prec > 0 ? 2.0 : 4.0;   // coarse coefficient
+    const double n0 = (double)d.n;
+    const double cell = 26.0 * cb + 4.0;      // coefficients + diagonal
+    double setup = 0.0, vc = 0.0;
+    if (d.nlev > 1) {
+        setup += n0 * (kb + 1.0) + (double)d.lev[1].n * cell;
+        for (int l = 1; l < d.nlev - 1; l++) setup += (double)d.lev[l].n * cell + (double)d.lev[l + 1].n * cell;
+        vc += 2.0 * nu * n0 * (kb + 1.0 + 8.0 + 4.0);          // fine GS sweeps: kappa, type, z rw, r
+        vc += n0 * (kb + 1.0 + 4.0 + 4.0) + (double)d.lev[1].n * 8.0;  // residual + restriction
+        vc += n0 * (1.0 + 8.0) + (double)d.lev[1].n * 4.0;    // prolongation
+        for (int l = 1; l < d.nlev - 1; l++) {
+            const double nl = (double)d.lev[l].n;
+            vc += 2.0 * nu * nl * (cell + 4.0 + 8.0);
+            vc += nl * (cell + 8.0) + (double)d.lev[l + 1].n * 8.0;
+            vc += nl * (4.0 + 8.0) + (double)d.lev[l + 1].n * 4.0;
+        }
+        vc += 2.0 * coarse_sweeps * (double)d.lev[d.nlev - 1].n * (cell + 4.0 + 8.0);
+    } else {
+        vc += 2.0 * coarse_sweeps * n0 * (kb + 1.0 + 8.0 + 4.0);
+    }
+    const double outer_res = n0 * (4.0 + 8.0 + 4.0 + 1.0 + 12.0);  // kappa, x64, b, type; r, e, z
+    const double accumulate = n0 * (16.0 + 4.0);
+    const double matvec = n0 * 13.0, update = n0 * 24.0, dot = n0 * 8.0, pupd = n0 * 16.0;
+    const int outer = d.outer_iters + 1;                // residual evaluations
+    const int corrections = d.outer_iters;              // inner solves
+    // each correction: V-cycle + r.z + p-update before its first iteration and
+    // after every iteration but the last, i.e. once per inner iteration overall
+    double b = setup + outer * outer_res + corrections * accumulate;
+    b += (double)d.inner_iters * (matvec + update + vc + dot + pupd);
+    return b;
+}
 }  // namespace
 
 pfsf_result Engine::register_kappa(int32_t id, const pfsf_island_kappa_buffers* b) {
@@ -75,6 +112,10 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
         }
         A->desc.push_back(d);
         A->ids.push_back(s->id);
+        const uint8_t* t = static_cast<const uint8_t*>(s->hosts.k_type);
+        int64_t act = 0;
+        for (int64_t i = 0; i < s->n; i++) act += t[i] == 1;
+        A->active.push_back(act);
     }
     if (coarse == 0) coarse = kAlignElems;
     A->nfine = fine;
@@ -206,6 +247,7 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
         launches_++;
     }
     cudaEventRecord(ev[1], stream_);
+    if (flags & PFSF_SOLVE_COLD_START) cudaMemsetAsync(k.x64, 0, (size_t)A.nfine * 8, stream_);
     int64_t nl = 0;
     std::vector<KDesc> res(set.size());
     if (batched) {
@@ -239,10 +281,14 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     cudaEventElapsedTime(&t_rb, ev[2], ev[3]);
     for (auto& e : ev) cudaEventDestroy(e);
     st.islands_solved = (int32_t)set.size();
-    for (const KDesc& d : res) {
+    for (size_t q = 0; q < res.size(); q++) {
+        const KDesc& d = res[q];
         st.islands_converged += d.converged ? 1 : 0;
         st.max_iterations = std::max(st.max_iterations, d.inner_iters);
         st.max_rel_residual = std::max(st.max_rel_residual, d.relres);
+        st.inner_iterations_total += d.inner_iters;
+        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps);
+        st.active_voxels += A.active[q];
     }
     st.device_ms = t_solve;
     st.upload_ms = t_up;

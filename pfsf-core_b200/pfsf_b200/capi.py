@@ -19,7 +19,7 @@ PFSF_OK, PFSF_ERROR_VULKAN, PFSF_ERROR_NO_DEVICE, PFSF_ERROR_OUT_OF_VRAM = 0, -1
 PFSF_ERROR_INVALID_ARG, PFSF_ERROR_NOT_INIT, PFSF_ERROR_ISLAND_FULL = -4, -5, -6
 PREC_FP32, PREC_BF16, PREC_FP16 = 0, 1, 2
 SOLVE_PER_ISLAND, SOLVE_BATCHED = 0, 1
-SOLVE_NO_UPLOAD, SOLVE_NO_READBACK = 0x1, 0x2
+SOLVE_NO_UPLOAD, SOLVE_NO_READBACK, SOLVE_COLD_START = 0x1, 0x2, 0x4
 
 
 class Pos(C.Structure):
@@ -78,7 +78,9 @@ class KappaBuffers(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("struct_bytes", C.c_int32), ("islands_solved", C.c_int32), ("islands_converged", C.c_int32),
                 ("max_iterations", C.c_int32), ("max_rel_residual", C.c_double), ("device_ms", C.c_float),
-                ("upload_ms", C.c_float), ("readback_ms", C.c_float), ("kernel_launches", C.c_int32)]
+                ("upload_ms", C.c_float), ("readback_ms", C.c_float), ("kernel_launches", C.c_int32),
+                ("inner_iterations_total", C.c_int64), ("algorithmic_bytes", C.c_double),
+                ("active_voxels", C.c_int64)]
 
 
 _lib = None
