@@ -93,6 +93,31 @@ PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine engine, int32_t island_id,
 PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine engine, int32_t island_id, int32_t field, void* out,
                                            int64_t bytes, int64_t* out_bytes);
 
+/* No counterpart in the reference ABI.  Failure-flag compaction that
+ * allocates nothing, for callers that cannot call cudaMalloc / cudaFree (a
+ * physics thread whose tick budget cannot absorb the device-wide
+ * synchronisation those calls may cause, or code that only borrows device
+ * buffers it does not own).  It runs the compaction pfsf_tick_dbb uses --
+ * failure flags (uint8 x lx*ly*lz, on the device) to {x, y, z, type} int32
+ * tuples in voxel order, world coordinates = origin + local -- with its
+ * per-chunk scratch in a fixed array inside the library (128 KiB per GPU,
+ * held until the process exits) instead of engine-allocated memory.
+ *   dev_fail_flags, dev_tuples (capacity x 4 int32), dev_count (1 int32):
+ *   device memory owned by the caller.  *dev_count receives the number of
+ *   failed voxels, which may exceed capacity; tuples past capacity are
+ *   dropped.
+ *   stream: a cudaStream_t (NULL = legacy default stream); the call only
+ *   enqueues work, the caller synchronises before reading the outputs.
+ * Limits and rules: islands above 67,108,864 voxels are rejected with
+ * PFSF_ERROR_INVALID_ARG.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and caches it; make that
+ * first call before any stream capture.  All calls on a device share the one
+ * array, so calls whose GPU work overlaps (different streams, no ordering)
+ * race and corrupt each other's results; serialise them. */
+PFSF_API pfsf_result pfsf_compact_failures_noalloc(const uint8_t* dev_fail_flags, int32_t lx, int32_t ly,
+                                                   int32_t lz, pfsf_pos origin, int32_t* dev_tuples,
+                                                   int32_t capacity, int32_t* dev_count, void* stream);
+
 /* The cudaStream_t the engine launches on (for event timing by callers). */
 PFSF_API void* pfsf_get_stream(pfsf_engine engine);
 

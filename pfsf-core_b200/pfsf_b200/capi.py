@@ -126,6 +126,8 @@ def load():
                                      C.POINTER(SolveStats)], C.c_int),
         "pfsf_read_solution64": ([E, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
         "pfsf_debug_read_field": ([E, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_compact_failures_noalloc": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, Pos, C.c_void_p, C.c_int32,
+                                           C.c_void_p, C.c_void_p], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
     }
