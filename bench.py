@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
 
@@ -317,7 +318,7 @@ def run_ours(args):
         plain_ms = stp.device_ms * len(isls) / len(sample)
         plain_note = (f"{len(sample)} of {len(isls)} islands (size-stratified), {stp.device_ms:.1f} ms, "
                       f"converged {stp.islands_converged}/{len(sample)}, scaled by island count")
-    cb = cpu_baseline(isls, args.cpu_seconds, args.tol) if (rank == 0 and ws == 1) else None
+    cb = cpu_baseline(isls, args.cpu_seconds, args.tol) if (rank == 0 and ws == 1 and not args.no_cpu) else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": "ms/tick", "n_gpus": ws, "steps": args.steps,
@@ -343,6 +344,12 @@ def run_ours(args):
             "plain_fp32_ms_per_tick": plain_ms, "plain_fp32_sample": plain_note,
             "speedup_vs_plain_fp32": (plain_ms / ms) if plain_ms else None,
             "inner_iterations_total": int(stats[-1].inner_iterations_total),
+            "schedule": {"island_ms_sum": stats[-1].island_ms_sum, "island_ms_max": stats[-1].island_ms_max,
+                         "span_ms": stats[-1].span_ms,
+                         "cluster": os.environ.get("PFSF_CLUSTER", "16"),
+                         "cluster_min_voxels": os.environ.get("PFSF_CLUSTER_MIN_VOXELS", "131072"),
+                         "warp_max_voxels": os.environ.get("PFSF_WARP_MAX_VOXELS", "0"),
+                         "smoother": os.environ.get("PFSF_SMOOTHER", "chebyshev(batched)"), "cheb_k": os.environ.get("PFSF_CHEB_K", "3")},
         }
         print(json.dumps(line), flush=True)
     eng.close()

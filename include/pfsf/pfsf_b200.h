@@ -61,6 +61,9 @@ typedef struct pfsf_solve_stats {
     double algorithmic_bytes;       /* compulsory bytes of every pass the solve made:
                                        each array a pass touches counted once per pass */
     int64_t active_voxels;          /* solid voxels over all solved islands */
+    double island_ms_sum;           /* batched mode: sum over islands of solve time */
+    double island_ms_max;           /* batched mode: longest single island solve */
+    double span_ms;                 /* batched mode: first island start to last island end */
 } pfsf_solve_stats;
 
 /* Registers the kappa-form inputs of an island created by pfsf_add_island.

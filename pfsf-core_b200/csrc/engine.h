@@ -195,6 +195,11 @@ private:
     struct Arena;
     std::unique_ptr<Arena> arena_;
     int num_sms_ = 148;
+    int64_t cluster_min_voxels_ = 131072;  // PFSF_CLUSTER_MIN_VOXELS
+    int cluster_size_ = 16;               // PFSF_CLUSTER (16, 8 or 1)
+    int64_t warp_max_voxels_ = 0;         // PFSF_WARP_MAX_VOXELS (0: no warp tier)
+    int smoother_ = -1;                   // PFSF_SMOOTHER (-1: mode default)
+    int cheb_k_ = 3;                      // PFSF_CHEB_K
 };
 
 }  // namespace pfsf_b200

@@ -24,6 +24,7 @@ struct KDesc {
     double relres;
     double bnorm;
     int inner_iters, outer_iters, converged, status;
+    unsigned long long t_start, t_end;  // %globaltimer (ns) around the island's solve
 };
 
 // Device pointers and parameters of one batched solve.
@@ -52,6 +53,14 @@ struct KArena {
     int fp64_dots;         // inner products in FP64 (1) or FP32 (0)
     float* scratch;        // plain mode: block partials + scalars (device)
     float* hscratch;       // plain mode: pinned host scalars
+    // Chebyshev smoother (smoother == 1): fine-level inverse diagonal and
+    // update vectors, coarse update vector, per-step coefficients
+    float* dinv0;
+    float* d0;
+    float* cd;
+    int smoother;          // 0 symmetric 8-colour Gauss-Seidel, 1 Chebyshev
+    int cheb_k;            // polynomial degree (stencil passes per smoothing)
+    float cheb_c1[4], cheb_c2[4];
 };
 
 struct KappaState {
@@ -65,8 +74,11 @@ struct KappaState {
 namespace kappa {
 // Plans levels for an island (host).
 int plan_levels(int lx, int ly, int lz, KLevel* lev);
-// Batched solve: one persistent launch over all islands in arena.
-void launch_batched(cudaStream_t s, const KArena& a, int ctas, int threads);
+// Batched solve: one persistent launch over all islands in the arena; the
+// first nbig islands of a.order are solved by thread-block clusters of
+// `cluster` CTAs (16, 8 or 1), the last nsmall by single warps, the rest by
+// single CTAs.  Returns 0 on success.
+int launch_batched(cudaStream_t s, const KArena& a, int nbig, int nsmall, int cluster, int num_sms);
 // Prepare kernels: sanitise kappa, round to 16-bit, zero non-solid source.
 void launch_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total, const int64_t* dummy);
 // Per-island plain solve driven from the host (one kernel per operation).

@@ -1,0 +1,424 @@
+// Batched tolerance solve: one persistent launch solves every island.
+//
+// Work distribution.  Islands are ordered largest first.  The kernel is
+// launched with thread-block clusters of C CTAs (C = 1 disables the cluster
+// phase).  Phase 1: each cluster takes the next "big" island from a queue
+// and its C CTAs solve it together -- cluster barriers (barrier.cluster,
+// release/acquire at cluster scope) between dependent passes, inner products
+// reduced across the cluster through distributed shared memory.  Phase 2:
+// when the big queue is empty every CTA independently takes small islands
+// from a second queue and solves each with CTA barriers only.  No grid-wide
+// synchronisation exists anywhere, so there is nothing to wait on across
+// clusters, and every island carries its own convergence state.
+//
+// Each island's solve: Galerkin hierarchy build, then outer FP64 refinement
+// around an inner FP32 PCG preconditioned by one V-cycle (see kappa_ops.cuh).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "kappa_ops.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace pfsf_b200 {
+namespace kappa {
+namespace {
+
+// 512 threads, two CTAs (two islands) per SM: the passes are latency bound
+// (L2 round trips between CTA barriers), so warps per SM matter more than
+// registers per thread (measured: 256 x 2 with 128 registers took 1.8x longer).
+constexpr int kBatchedThreads = 512;
+constexpr int kBatchedMinBlocks = 2;
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct SharedScratch {
+    double shd[34];
+    float shf[34];
+    double slotd[2][16];
+    float slotf[2][16];
+    int next;
+};
+
+// Team = one CTA.
+struct CtaTeam {
+    SharedScratch* sh;
+    __device__ int64_t t() const { return threadIdx.x; }
+    __device__ int64_t T() const { return blockDim.x; }
+    __device__ bool leader() const { return threadIdx.x == 0; }
+    __device__ bool leader_warp() const { return threadIdx.x < 32; }
+    __device__ void sync() const { __syncthreads(); }
+    __device__ double sum(double v) { return cta_sum(v, sh->shd); }
+    __device__ float sum(float v) { return cta_sum(v, sh->shf); }
+};
+
+// Team = one warp (small islands): warp barriers only, shuffle reductions.
+struct WarpTeam {
+    __device__ int64_t t() const { return threadIdx.x & 31; }
+    __device__ int64_t T() const { return 32; }
+    __device__ bool leader() const { return (threadIdx.x & 31) == 0; }
+    __device__ bool leader_warp() const { return true; }
+    __device__ void sync() const { __syncwarp(); }
+    __device__ double sum(double v) { return __shfl_sync(0xffffffffu, warp_sum(v), 0); }
+    __device__ float sum(float v) { return __shfl_sync(0xffffffffu, warp_sum(v), 0); }
+};
+
+// Team = thread-block cluster of C CTAs.  Inner products: CTA reduction, then
+// each CTA's partial is written into rank 0's shared slots (double-buffered
+// by call parity, so one cluster barrier per reduction suffices) and summed in
+// rank order by every CTA -- identical, deterministic results everywhere.
+template <int C>
+struct ClusterTeam {
+    SharedScratch* sh;
+    int parity = 0;
+    __device__ int64_t t() const { return (int64_t)cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
+    __device__ int64_t T() const { return (int64_t)C * blockDim.x; }
+    __device__ bool leader() const { return cg::this_cluster().block_rank() == 0 && threadIdx.x == 0; }
+    __device__ bool leader_warp() const { return cg::this_cluster().block_rank() == 0 && threadIdx.x < 32; }
+    __device__ void sync() const { cg::this_cluster().sync(); }
+    template <class R>
+    __device__ R xsum(R v, R* local, R (*slots)[16]) {
+        cg::cluster_group cl = cg::this_cluster();
+        const R part = cta_sum(v, local);
+        if (threadIdx.x == 0) {
+            R* dst = cl.map_shared_rank(&slots[parity][0], 0);
+            dst[cl.block_rank()] = part;
+        }
+        cl.sync();
+        if (threadIdx.x < 32) {
+            const R* src = cl.map_shared_rank(&slots[parity][0], 0);
+            R s = threadIdx.x < C ? src[threadIdx.x] : R(0);
+            s = warp_sum(s);
+            if (threadIdx.x == 0) local[33] = s;
+        }
+        __syncthreads();
+        parity ^= 1;
+        return local[33];
+    }
+    __device__ double sum(double v) { return xsum<double>(v, sh->shd, sh->slotd); }
+    __device__ float sum(float v) { return xsum<float>(v, sh->shf, sh->slotf); }
+};
+
+// One V-cycle z = M r.  Levels above kWarpTailCells cells are processed by
+// the whole team; from the first level at or below it the rest of the cycle
+// runs on one warp of the leader CTA (warp barriers only).
+template <int P, class TeamT>
+__device__ void team_vcycle(const KArena& A, const KDesc& D, TeamT& tm) {
+    const int t = (int)tm.t(), T = (int)tm.T();
+    const int L = D.nlev;
+    if (L <= 1) {
+        for (int s = 0; s < A.coarse_sweeps; s++) {
+            for (int c = 0; c < 8; c++) { op_smooth0<P>(A, D, t, T, c); tm.sync(); }
+            for (int c = 7; c >= 0; c--) { op_smooth0<P>(A, D, t, T, c); tm.sync(); }
+        }
+        return;
+    }
+    int l0 = 1;
+    while (l0 < L - 1 && D.lev[l0].n > kWarpTailCells) l0++;
+    for (int s = 0; s < A.nu; s++)
+        for (int c = 0; c < 8; c++) { op_smooth0<P>(A, D, t, T, c); tm.sync(); }
+    op_restrict0<P>(A, D, t, T);
+    tm.sync();
+    for (int l = 1; l < l0; l++) {
+        for (int s = 0; s < A.nu; s++)
+            for (int c = 0; c < 8; c++) { op_smoothc<P>(A, D, l, t, T, c); tm.sync(); }
+        op_restrictc<P>(A, D, l, t, T);
+        tm.sync();
+    }
+    if (D.lev[l0].n <= kWarpTailCells) {
+        if (tm.leader_warp()) warp_tail_vcycle<P>(A, D, l0, A.nu, A.coarse_sweeps, A.omega_c);
+        tm.sync();
+    } else {  // coarsest level still large: team sweeps
+        for (int s = 0; s < A.coarse_sweeps; s++) {
+            for (int c = 0; c < 8; c++) { op_smoothc<P>(A, D, L - 1, t, T, c); tm.sync(); }
+            for (int c = 7; c >= 0; c--) { op_smoothc<P>(A, D, L - 1, t, T, c); tm.sync(); }
+        }
+    }
+    for (int l = l0 - 1; l >= 1; l--) {
+        op_prolongc(A, D, l, t, T, A.omega_c);
+        tm.sync();
+        for (int s = 0; s < A.nu; s++)
+            for (int c = 7; c >= 0; c--) { op_smoothc<P>(A, D, l, t, T, c); tm.sync(); }
+    }
+    op_prolong0(A, D, t, T, A.omega_c);
+    tm.sync();
+    for (int s = 0; s < A.nu; s++)
+        for (int c = 7; c >= 0; c--) { op_smooth0<P>(A, D, t, T, c); tm.sync(); }
+}
+
+// Chebyshev smoothing of degree A.cheb_k on the fine level (from z = 0 when
+// `from_zero`), two passes per step.
+template <int P, class TeamT>
+__device__ void team_cheb0(const KArena& A, const KDesc& D, TeamT& tm, bool from_zero) {
+    const int t = (int)tm.t(), T = (int)tm.T();
+    int j = 0;
+    if (from_zero) {
+        op_cheb0_first(A, D, t, T, A.cheb_c2[0]);
+        tm.sync();
+        j = 1;
+    }
+    for (; j < A.cheb_k; j++) {
+        op_cheb0_d<P>(A, D, t, T, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
+        tm.sync();
+        op_cheb0_z(A, D, t, T);
+        tm.sync();
+    }
+}
+template <int P, class TeamT>
+__device__ void team_chebc(const KArena& A, const KDesc& D, int l, TeamT& tm, bool from_zero) {
+    const int t = (int)tm.t(), T = (int)tm.T();
+    int j = 0;
+    if (from_zero) {
+        op_chebc_first(A, D, l, t, T, A.cheb_c2[0]);
+        tm.sync();
+        j = 1;
+    }
+    for (; j < A.cheb_k; j++) {
+        op_chebc_d<P>(A, D, l, t, T, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
+        tm.sync();
+        op_chebc_x(A, D, l, t, T);
+        tm.sync();
+    }
+}
+
+// V-cycle with Chebyshev smoothing on the team levels (same structure as
+// team_vcycle; the single-warp tail keeps Gauss-Seidel).
+template <int P, class TeamT>
+__device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
+    const int t = (int)tm.t(), T = (int)tm.T();
+    const int L = D.nlev;
+    if (L <= 1) {
+        team_cheb0<P>(A, D, tm, true);
+        team_cheb0<P>(A, D, tm, false);
+        return;
+    }
+    int l0 = 1;
+    while (l0 < L - 1 && D.lev[l0].n > kWarpTailCells) l0++;
+    team_cheb0<P>(A, D, tm, true);
+    op_restrict0<P>(A, D, t, T);
+    tm.sync();
+    for (int l = 1; l < l0; l++) {
+        team_chebc<P>(A, D, l, tm, true);
+        op_restrictc<P>(A, D, l, t, T);
+        tm.sync();
+    }
+    if (D.lev[l0].n <= kWarpTailCells) {
+        if (tm.leader_warp()) warp_tail_vcycle<P>(A, D, l0, A.nu, A.coarse_sweeps, A.omega_c);
+        tm.sync();
+    } else {
+        team_chebc<P>(A, D, L - 1, tm, true);
+        for (int s = 1; s < A.coarse_sweeps; s++) team_chebc<P>(A, D, L - 1, tm, false);
+    }
+    for (int l = l0 - 1; l >= 1; l--) {
+        op_prolongc(A, D, l, t, T, A.omega_c);
+        tm.sync();
+        team_chebc<P>(A, D, l, tm, false);
+    }
+    op_prolong0(A, D, t, T, A.omega_c);
+    tm.sync();
+    team_cheb0<P>(A, D, tm, false);
+}
+
+template <int P, class TeamT>
+__device__ __forceinline__ void precondition(const KArena& A, const KDesc& D, TeamT& tm) {
+    if (A.smoother == 1) team_vcycle_cheb<P>(A, D, tm);
+    else team_vcycle<P>(A, D, tm);
+}
+
+template <int P, class R, class TeamT>
+__device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
+    const int t = (int)tm.t(), T = (int)tm.T();
+    const unsigned long long t0 = globaltimer();
+    if (D.nlev > 1) {
+        op_build1<P>(A, D, t, T);
+        tm.sync();
+        for (int l = 1; l < D.nlev - 1; l++) {
+            op_buildc<P>(A, D, l, t, T);
+            tm.sync();
+        }
+    }
+    if (A.smoother == 1) {
+        op_dinv0<P>(A, D, t, T);
+        tm.sync();
+    }
+    double relres = 1.0, bn = 0.0;
+    int inner_total = 0, outer = 0;
+    bool conv = false;
+    for (outer = 0; outer <= A.max_outer; outer++) {
+        double rr = 0.0, bb = 0.0;
+        op_outer_residual(A, D, t, T, rr, bb);
+        rr = tm.sum(rr);
+        bb = tm.sum(bb);
+        bn = sqrt(bb);
+        relres = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+        if (relres <= A.tol) { conv = true; break; }
+        if (outer == A.max_outer || inner_total >= A.max_inner) break;
+        // inner PCG on A e = r, stopping at ||r_in|| <= eta ||r_out||
+        const double eta = fmax(A.eta_min, 0.3 * A.tol / relres);
+        const R stop2 = (R)(eta * eta * rr);
+        precondition<P>(A, D, tm);
+        R rz = 0;
+        op_dot_rz(A, D, t, T, rz);
+        rz = tm.sum(rz);
+        op_pupdate(A, D, t, T, 0.0f);
+        tm.sync();
+        for (int it = 0; it < A.max_inner - inner_total; it++) {
+            R pq = 0;
+            op_matvec(A, D, t, T, pq);
+            pq = tm.sum(pq);
+            const float alpha = pq > (R)0 ? (float)(rz / pq) : 0.0f;
+            R rri = 0;
+            op_update(A, D, t, T, alpha, rri);
+            rri = tm.sum(rri);
+            inner_total++;
+            if (rri <= stop2 || !(pq > (R)0)) break;
+            precondition<P>(A, D, tm);
+            R rzn = 0;
+            op_dot_rz(A, D, t, T, rzn);
+            rzn = tm.sum(rzn);
+            const float beta = rz > (R)0 ? (float)(rzn / rz) : 0.0f;
+            rz = rzn;
+            op_pupdate(A, D, t, T, beta);
+            tm.sync();
+        }
+        op_accumulate(A, D, t, T);
+        tm.sync();
+    }
+    if (tm.leader()) {
+        D.relres = relres;
+        D.bnorm = bn;
+        D.inner_iters = inner_total;
+        D.outer_iters = outer;
+        D.converged = conv ? 1 : 0;
+        D.t_start = t0;
+        D.t_end = globaltimer();
+    }
+}
+
+// queue[0]: big islands taken by clusters; queue[1]: small islands taken by CTAs.
+template <int P, int C>
+__global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
+    k_batched(const __grid_constant__ KArena A, int nbig, int nsmall) {
+    __shared__ SharedScratch sh;
+    if constexpr (C > 1) {
+        cg::cluster_group cl = cg::this_cluster();
+        ClusterTeam<C> tm{&sh};
+        for (;;) {
+            if (cl.block_rank() == 0 && threadIdx.x == 0) sh.next = atomicAdd(&A.queue[0], 1);
+            cl.sync();
+            const int q = *cl.map_shared_rank(&sh.next, 0);
+            if (q >= nbig) break;
+            KDesc& D = A.desc[A.order[q]];
+            if (A.fp64_dots) team_solve<P, double>(A, D, tm);
+            else team_solve<P, float>(A, D, tm);
+            cl.sync();
+        }
+        cl.sync();  // no CTA leaves while a peer may still read its shared memory
+    }
+    CtaTeam tm{&sh};
+    const int nmid_end = A.nisl - nsmall;
+    for (;;) {
+        if (threadIdx.x == 0) sh.next = atomicAdd(&A.queue[1], 1);
+        __syncthreads();
+        const int q = nbig + sh.next;
+        __syncthreads();
+        if (q >= nmid_end) break;
+        KDesc& D = A.desc[A.order[q]];
+        if (A.fp64_dots) team_solve<P, double>(A, D, tm);
+        else team_solve<P, float>(A, D, tm);
+        __syncthreads();
+    }
+    // small islands: every warp on its own, no CTA barrier from here on
+    WarpTeam wt;
+    for (;;) {
+        int k = 0;
+        if ((threadIdx.x & 31) == 0) k = atomicAdd(&A.queue[2], 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        const int q = nmid_end + k;
+        if (q >= A.nisl) break;
+        KDesc& D = A.desc[A.order[q]];
+        if (A.fp64_dots) team_solve<P, double>(A, D, wt);
+        else team_solve<P, float>(A, D, wt);
+        __syncwarp();
+    }
+}
+
+template <int P, int C>
+cudaError_t launch_one(cudaStream_t s, const KArena& a, int nbig, int nsmall, int num_sms) {
+    auto kern = k_batched<P, C>;
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    cfg.blockDim = dim3(kBatchedThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    int per_sm = kBatchedMinBlocks;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, 0) != cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    int ctas = num_sms * per_sm;
+    if (C > 1) {
+        if (C > 8) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cfg.gridDim = dim3(C);
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters <= 0) {
+            cudaGetLastError();
+            return cudaErrorInvalidConfiguration;
+        }
+        ctas = clusters * C;
+    } else {
+        cfg.attrs = nullptr;
+        cfg.numAttrs = 0;
+    }
+    cfg.gridDim = dim3(std::max(C, std::min(ctas, std::max(C, a.nisl * C))));
+    return cudaLaunchKernelEx(&cfg, kern, a, nbig, nsmall);
+}
+
+template <int P>
+cudaError_t launch_p(cudaStream_t s, const KArena& a, int nbig, int nsmall, int cluster, int num_sms) {
+    if (nbig > 0 && cluster >= 16) {
+        if (launch_one<P, 16>(s, a, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
+        cudaGetLastError();
+    }
+    if (nbig > 0 && cluster >= 8) {
+        if (launch_one<P, 8>(s, a, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
+        cudaGetLastError();
+    }
+    return launch_one<P, 1>(s, a, 0, nsmall, num_sms);
+}
+
+}  // namespace
+
+int batched_threads() { return kBatchedThreads; }
+
+// nbig: number of leading islands (in a.order) solved by whole clusters;
+// nsmall: number of trailing islands solved by single warps.
+int launch_batched(cudaStream_t s, const KArena& a, int nbig, int nsmall, int cluster, int num_sms) {
+    cudaError_t e;
+    switch (a.prec) {
+        case 1: e = launch_p<1>(s, a, nbig, nsmall, cluster, num_sms); break;
+        case 2: e = launch_p<2>(s, a, nbig, nsmall, cluster, num_sms); break;
+        default: e = launch_p<0>(s, a, nbig, nsmall, cluster, num_sms); break;
+    }
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "[libpfsf] batched solve launch failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    return 0;
+}
+
+}  // namespace kappa
+}  // namespace pfsf_b200

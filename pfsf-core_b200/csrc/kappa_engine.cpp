@@ -21,27 +21,36 @@ inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 // Compulsory bytes of the passes one island's solve made: every array a pass
 // reads or writes counted once per pass (what a perfectly cached streaming
 // implementation must move), per grid voxel / coarse cell.
-double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps) {
+double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps, int smoother, int cheb_k) {
     const double kb = prec > 0 ? 2.0 : 4.0;   // preconditioner kappa
     const double cb = prec > 0 ? 2.0 : 4.0;   // coarse coefficient
+    const double wf = kb;                     // fine-level weights come from kappa
     const double n0 = (double)d.n;
     const double cell = 26.0 * cb + 4.0;      // coefficients + diagonal
     double setup = 0.0, vc = 0.0;
     if (d.nlev > 1) {
-        setup += n0 * (kb + 1.0) + (double)d.lev[1].n * cell;
+        setup += n0 * (wf + 1.0) + (double)d.lev[1].n * cell;
         for (int l = 1; l < d.nlev - 1; l++) setup += (double)d.lev[l].n * cell + (double)d.lev[l + 1].n * cell;
-        vc += 2.0 * nu * n0 * (kb + 1.0 + 8.0 + 4.0);          // fine GS sweeps: kappa, type, z rw, r
-        vc += n0 * (kb + 1.0 + 4.0 + 4.0) + (double)d.lev[1].n * 8.0;  // residual + restriction
+        if (smoother == 1) {
+            // Chebyshev: first step (r, dinv -> d, z), then per step a stencil
+            // pass (weights, type, z, r, dinv, d rw) and an update pass (d, z rw, type)
+            const double step = (wf + 1.0 + 4.0 + 4.0 + 4.0 + 8.0) + (4.0 + 8.0 + 1.0);
+            vc += n0 * 16.0 + (2.0 * cheb_k - 1.0) * n0 * step;
+            setup += n0 * (wf + 1.0 + 4.0);  // inverse diagonal
+        } else {
+            vc += 2.0 * nu * n0 * (wf + 1.0 + 8.0 + 4.0);      // fine GS sweeps: weights, type, z rw, r
+        }
+        vc += n0 * (wf + 1.0 + 4.0 + 4.0) + (double)d.lev[1].n * 8.0;  // residual + restriction
         vc += n0 * (1.0 + 8.0) + (double)d.lev[1].n * 4.0;    // prolongation
         for (int l = 1; l < d.nlev - 1; l++) {
             const double nl = (double)d.lev[l].n;
-            vc += 2.0 * nu * nl * (cell + 4.0 + 8.0);
+            vc += (smoother == 1 ? (2.0 * cheb_k) * (cell + 4.0 + 8.0 + 8.0) : 2.0 * nu * (cell + 4.0 + 8.0)) * nl;
             vc += nl * (cell + 8.0) + (double)d.lev[l + 1].n * 8.0;
             vc += nl * (4.0 + 8.0) + (double)d.lev[l + 1].n * 4.0;
         }
         vc += 2.0 * coarse_sweeps * (double)d.lev[d.nlev - 1].n * (cell + 4.0 + 8.0);
     } else {
-        vc += 2.0 * coarse_sweeps * n0 * (kb + 1.0 + 8.0 + 4.0);
+        vc += 2.0 * coarse_sweeps * n0 * (wf + 1.0 + 8.0 + 4.0);
     }
     const double outer_res = n0 * (4.0 + 8.0 + 4.0 + 1.0 + 12.0);  // kappa, x64, b, type; r, e, z
     const double accumulate = n0 * (16.0 + 4.0);
@@ -129,7 +138,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
                  o_p = take(fine * 4), o_q = take(fine * 4), o_cd = take(coarse * 4), o_cf = take(coarse * 26 * cbytes),
                  o_cx = take(coarse * 4), o_cb = take(coarse * 4), o_desc = take(sizeof(KDesc) * nisl),
                  o_order = take(sizeof(int) * nisl), o_queue = take(256),
-                 o_scr = take(sizeof(float) * kappa::plain_scratch_floats());
+                 o_scr = take(sizeof(float) * kappa::plain_scratch_floats()), o_dinv = take(fine * 4),
+                 o_d0 = take(fine * 4), o_cdd = take(coarse * 4);
     A->bytes = off;
     if (fault_alloc_after_ >= 0 && alloc_count_ >= fault_alloc_after_) return false;
     if (cudaMalloc(&A->base, A->bytes) != cudaSuccess) {
@@ -163,6 +173,9 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     k.order = reinterpret_cast<int*>(b + o_order);
     k.queue = reinterpret_cast<int*>(b + o_queue);
     k.scratch = reinterpret_cast<float*>(b + o_scr);
+    k.dinv0 = reinterpret_cast<float*>(b + o_dinv);
+    k.d0 = reinterpret_cast<float*>(b + o_d0);
+    k.cd = reinterpret_cast<float*>(b + o_cdd);
     k.nisl = nisl;
     k.prec = A->prec;
     if (!CU_OK(cudaMallocHost((void**)&A->hscratch, 256))) return false;
@@ -224,6 +237,23 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     k.coarse_sweeps = 4;
     const bool batched = solve_mode_ == PFSF_SOLVE_BATCHED;
     k.fp64_dots = batched ? 1 : 0;
+    // batched: Chebyshev smoothing (one stencil pass per step, few barriers);
+    // plain: symmetric 8-colour Gauss-Seidel (the RBGS of the reference)
+    k.smoother = smoother_ >= 0 ? smoother_ : (batched ? 1 : 0);
+    k.cheb_k = std::max(1, std::min(4, cheb_k_));
+    {
+        const double lmax = 2.0, lmin = lmax * 0.1;
+        const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+        double rho = 1.0 / sigma;
+        k.cheb_c1[0] = 0.0f;
+        k.cheb_c2[0] = (float)(1.0 / theta);
+        for (int j = 1; j < 4; j++) {
+            const double rn = 1.0 / (2.0 * sigma - rho);
+            k.cheb_c1[j] = (float)(rn * rho);
+            k.cheb_c2[j] = (float)(2.0 * rn / delta);
+            rho = rn;
+        }
+    }
 
     cudaEvent_t ev[4];
     for (auto& e : ev) cudaEventCreate(&e);
@@ -251,10 +281,16 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     int64_t nl = 0;
     std::vector<KDesc> res(set.size());
     if (batched) {
-        cudaMemsetAsync(k.queue, 0, sizeof(int), stream_);
-        int per_sm = 2;
-        const int ctas = std::max(1, std::min((int)set.size(), num_sms_ * per_sm));
-        kappa::launch_batched(stream_, k, ctas, kappa::batched_threads());
+        cudaMemsetAsync(k.queue, 0, 4 * sizeof(int), stream_);
+        // islands at or above the cluster threshold are solved by whole
+        // thread-block clusters (largest first), islands below the warp
+        // threshold by single warps, the rest by single CTAs
+        int nbig = 0, nsmall = 0;
+        for (const KDesc& d : A.desc) {
+            nbig += d.n >= cluster_min_voxels_ ? 1 : 0;
+            nsmall += d.n < warp_max_voxels_ ? 1 : 0;
+        }
+        if (kappa::launch_batched(stream_, k, nbig, nsmall, cluster_size_, num_sms_) != 0) return PFSF_ERROR_VULKAN;
         nl = 1;
     } else {
         for (size_t q = 0; q < set.size(); q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &res[q]);
@@ -287,8 +323,19 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
         st.max_iterations = std::max(st.max_iterations, d.inner_iters);
         st.max_rel_residual = std::max(st.max_rel_residual, d.relres);
         st.inner_iterations_total += d.inner_iters;
-        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps);
+        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps, k.smoother, k.cheb_k);
         st.active_voxels += A.active[q];
+    }
+    if (batched) {
+        unsigned long long t0 = ~0ull, t1 = 0;
+        for (const KDesc& d : res) {
+            t0 = std::min(t0, d.t_start);
+            t1 = std::max(t1, d.t_end);
+            const double ms = (double)(d.t_end - d.t_start) * 1e-6;
+            st.island_ms_sum += ms;
+            st.island_ms_max = std::max(st.island_ms_max, ms);
+        }
+        st.span_ms = t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
     }
     st.device_ms = t_solve;
     st.upload_ms = t_up;
