@@ -988,7 +988,7 @@ int o_kappa_pcg64(int lx, int ly, int lz, const double *kappa, const uint8_t *ty
 double o_kappa_relres(int lx, int ly, int lz, const double *kappa, const uint8_t *type, const double *s,
                       const float *phi32) {
     int64_t n = (int64_t)lx * ly * lz;
-    double *x = malloc(n * 8), *q = malloc(n * 8);
+    double *x = calloc(n, 8), *q = calloc(n, 8);
     for (int64_t i = 0; i < n; i++) x[i] = type[i] == 1 ? (double)phi32[i] : 0.0;
     o_kappa_apply(lx, ly, lz, kappa, type, x, q);
     double rn = 0.0, bn = 0.0;
