@@ -14,7 +14,8 @@ extern "C" {
  * max(1, max conductivity) when it exceeds 1; reports sigma_max. */
 PFSF_API void pfsf_normalize_soa6(float* source, float* rcomp, float* rtens, float* conductivity,
                                   const float* hydration, int32_t n, float* out_sigma_max);
-/* Scale horizontal faces up (downwind) / down (upwind) by (1 + upwind_factor). */
+/* No-op kept for the ABI: the reference disabled the upwind face bias because
+ * it made the operator non-symmetric (wind enters through the source term). */
 PFSF_API void pfsf_apply_wind_bias(float* conductivity, int32_t n, pfsf_vec3 wind, float upwind_factor);
 PFSF_API float pfsf_timoshenko_moment_factor(float b, float h, int32_t arm, float youngs_gpa, float nu);
 PFSF_API float pfsf_wind_pressure_source(float wind_speed, float density_kg_m3, bool exposed);

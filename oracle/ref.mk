@@ -1,0 +1,27 @@
+# Builds the reference's own CPU primitives (test infrastructure only) from
+# their sources where they lie, into oracle/_ref/libpfsf_ref.so, so the
+# library's host exports can be checked against them bit for bit.
+#
+#   make -C oracle -f ref.mk
+#
+# Only the CPU translation units are used (compute/, ext/, trace/, diag/):
+# they need no Vulkan and no generated code.  Compiled without FMA
+# contraction and without -march, like this library's host code; the
+# reference's own build adds -march=x86-64-v3, whose FMA contraction the Java
+# side it mirrors does not have.  -Bsymbolic keeps the library's calls to
+# its own exports inside itself when it is loaded beside libpfsf.so.
+REF ?= /root/reference/L1-native/libpfsf
+OUT := _ref
+CXX ?= g++
+CXXFLAGS := -O2 -std=c++17 -fPIC -ffp-contract=off -w -I$(REF)/include -DPFSF_ABI_VERSION_STRING='"1.5.0"'
+SRCS := $(wildcard $(REF)/src/compute/*.cpp) $(REF)/src/ext/augmentation.cpp $(REF)/src/ext/hooks.cpp \
+        $(REF)/src/ext/plan_dispatcher.cpp $(REF)/src/trace/ring_buffer.cpp $(REF)/src/diag/crash.cpp
+
+all: $(OUT)/libpfsf_ref.so
+
+$(OUT)/libpfsf_ref.so: $(SRCS)
+	mkdir -p $(OUT)
+	$(CXX) $(CXXFLAGS) -shared -Wl,-Bsymbolic -o $@ $(SRCS) -lpthread
+
+clean:
+	rm -rf $(OUT)

@@ -27,7 +27,8 @@ CUDA_HOME = os.path.dirname(os.path.dirname(os.path.realpath(NVCC)))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-fvisibility=hidden",
               "-I" + INCLUDE, "-I" + CSRC, "-DPFSF_EXPORT"]
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-I" + INCLUDE, "-I" + CSRC,
+# host primitives keep the reference's rounding: no FMA contraction
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-Wall", "-I" + INCLUDE, "-I" + CSRC,
              "-I" + os.path.join(CUDA_HOME, "include"), "-DPFSF_EXPORT"]
 # per-file extra flags: the reference-schedule kernels round every product
 # and sum as written (no FMA contraction) so they track the FP32 restatement.
