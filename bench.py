@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch", "single"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "single", "adjoint"], default="batch")
+    ap.add_argument("--fd-voxels", type=int, default=256)
     ap.add_argument("--islands", type=int, default=4096)
     ap.add_argument("--target-active", type=float, default=6.0e7)
     ap.add_argument("--tol", type=float, default=1e-6)
@@ -239,7 +240,9 @@ def run_ours(args):
         host.append(h)
         ids.append(iid)
     prec = {"bf16": capi.PREC_BF16, "fp16": capi.PREC_FP16, "fp32": capi.PREC_FP32}[args.precision]
-    mode = capi.SOLVE_BATCHED if args.workload == "batch" else capi.SOLVE_PER_ISLAND
+    # the product path is the persistent launch in both workloads (a single
+    # giant island takes its whole-GPU tier); the plain arm is per-island FP32
+    mode = capi.SOLVE_BATCHED
     eng.set_solve_mode(mode)
     eng.set_precision(prec)
     rc, st0 = eng.solve(ids, tol=args.tol, flags=capi.SOLVE_COLD_START)  # builds and uploads the arena
@@ -290,26 +293,38 @@ def run_ours(args):
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
     tm = traffic_model()
     traffic = None
-    if tm and tm.get("dram_bytes_per_active_voxel"):
+    if tm and tm.get("dram_bytes_per_active_voxel") and mode == capi.SOLVE_BATCHED:
         traffic = tm["dram_bytes_per_active_voxel"] * st0.active_voxels
-    # FP64-oracle error on a few islands (read the FP64 accumulator back)
+    # FP64-oracle error on a few islands (read the FP64 accumulator back).
+    # The single 256x256x128 island is too large for the CPU FP64 solve
+    # (hours single-threaded); for it the oracle evaluates the relative
+    # residual of the returned FP64 solution with its own FP64 operator.
     oracle_err = None
+    oracle_relres = None
     if rank == 0:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
-        errs = []
+        errs, rels = [], []
         for k in stratified(isls, 4):
+            isl = isls[k]
+            rc, x64 = eng.read_solution64(ids[k], isl.n)
+            k64 = isl.kappa.astype(np.float64)
+            r = isl.source.astype(np.float64) - O.kappa_apply(isl.dims, k64, isl.vtype, x64)
+            solid = isl.vtype == 1
+            rels.append(float(np.linalg.norm(r[solid]) / np.linalg.norm(isl.source[solid].astype(np.float64))))
+        oracle_relres = max(rels)
+        for k in ([] if args.workload == "single" else stratified(isls, 4)):
             isl = isls[k]
             rc, x64 = eng.read_solution64(ids[k], isl.n)
             xr, _, _ = O.kappa_solve64(isl.dims, isl.kappa.astype(np.float64), isl.vtype,
                                        isl.source.astype(np.float64), tol=1e-12, maxit=200000)
             errs.append(float(np.abs(x64 - xr).max() / max(np.abs(xr).max(), 1e-300)))
-        oracle_err = max(errs)
+        oracle_err = max(errs) if errs else None
     # plain FP32 per-island kernels on a stratified sample
     plain_ms = None
     plain_note = None
-    if not args.no_plain and args.workload == "batch" and rank == 0:
-        sample = stratified(isls, args.plain_sample)
+    if not args.no_plain and rank == 0:
+        sample = stratified(isls, args.plain_sample) if args.workload == "batch" else [0]
         sids = [ids[k] for k in sample]
         eng.set_solve_mode(capi.SOLVE_PER_ISLAND)
         eng.set_precision(capi.PREC_FP32)
@@ -318,14 +333,18 @@ def run_ours(args):
         plain_ms = stp.device_ms * len(isls) / len(sample)
         plain_note = (f"{len(sample)} of {len(isls)} islands (size-stratified), {stp.device_ms:.1f} ms, "
                       f"converged {stp.islands_converged}/{len(sample)}, scaled by island count")
-    cb = cpu_baseline(isls, args.cpu_seconds, args.tol) if (rank == 0 and ws == 1 and not args.no_cpu) else None
+    # the CPU FP64 solve of the single 5 M-voxel island does not fit a bounded sample
+    cb = (cpu_baseline(isls, args.cpu_seconds, args.tol)
+          if (rank == 0 and ws == 1 and not args.no_cpu and args.workload == "batch") else None)
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": "ms/tick", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": (f"{len(isls)} islands/GPU (log-uniform sides, scale {meta['scale']:.3f}), "
-                                    f"{meta['grid_total']} grid / {meta['active_total']} active voxels, "
+            "config": {"workload": ((f"{len(isls)} islands/GPU (log-uniform sides, scale {meta['scale']:.3f}), "
+                                     if args.workload == "batch" else
+                                     "one 256x256x128 noise island (60 % occupancy, anchored component), ")
+                                    + f"{meta['grid_total']} grid / {meta['active_total']} active voxels, "
                                     f"cold start, tol {args.tol:g}"),
                        "islands": len(isls), "grid_voxels": meta["grid_total"], "active_voxels": meta["active_total"],
                        "mode": "batched persistent" if mode == capi.SOLVE_BATCHED else "per-island",
@@ -334,13 +353,14 @@ def run_ours(args):
             "e2e": {"value": e2e_ms, "unit": "ms/tick", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_batched (persistent solve)", "kernel_ms": kern_ms,
+                         "kernel": ("k_batched (persistent solve)" if args.workload == "batch"
+                                    else "k_grid (whole-GPU persistent solve)"), "kernel_ms": kern_ms,
                          "algorithmic_bytes": alg_bytes},
             "cpu_baseline": cb,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "converged": f"{conv}/{len(isls)}", "max_rel_residual_fp64": maxrel,
-            "fp64_oracle_error": oracle_err,
+            "fp64_oracle_error": oracle_err, "fp64_oracle_relres": oracle_relres,
             "plain_fp32_ms_per_tick": plain_ms, "plain_fp32_sample": plain_note,
             "speedup_vs_plain_fp32": (plain_ms / ms) if plain_ms else None,
             "inner_iterations_total": int(stats[-1].inner_iterations_total),
@@ -357,10 +377,88 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_adjoint(args):
+    """Calibration gradient on one 128x128x64 noise island: 32 ticks with the
+    load ramped linearly to 2x (checkpoint every 8 ticks), loss
+    L = sum softplus(flux_in / rcomp - 1) + 1/2 ||phi - phi_target||^2 at the
+    last tick (rcomp in Pa: flux in N over a 1 m^2 face), phi_target = the
+    solution for kappa perturbed by a seeded lognormal (sigma 0.2) factor.
+    Reports ms per forward tick, ms of the backward (adjoint solve + edge
+    product), and the adjoint gradient's error against central finite
+    differences (h = 2^-10 on kappa) at --fd-voxels random voxels."""
+    os.environ.setdefault("PFSF_GRID_MIN_VOXELS", str(1 << 18))  # a lone island takes the whole GPU
+    from pfsf_b200 import adjoint as AD
+    from pfsf_b200 import capi, synth
+    import torch
+
+    isl = synth.noise_island((128, 128, 64), seed=41)
+    rng = np.random.default_rng(41)
+    eng = capi.Engine(capi.default_config(max_island_size=1 << 28, tick_budget_ms=1 << 30, vram=180 << 30))
+    if eng.init() != capi.PFSF_OK:
+        raise RuntimeError("pfsf_init failed")
+    eng.set_solve_mode(capi.SOLVE_BATCHED)
+    eng.set_precision({"bf16": capi.PREC_BF16, "fp16": capi.PREC_FP16, "fp32": capi.PREC_FP32}[args.precision])
+    sess = AD.Session(eng, 1, isl.dims, isl.vtype, tol=1e-10, max_iter=4000)
+    ticks = 32
+    k_target = (isl.kappa * np.exp(0.2 * rng.standard_normal(isl.n))).astype(np.float32)
+    phi_target = sess.solve(k_target, (2.0 * isl.source).astype(np.float32))
+    rcomp = torch.tensor(np.maximum(isl.rcomp.astype(np.float64), 1.0) * 1e6)
+    pt = torch.tensor(phi_target)
+    kt = torch.tensor(isl.kappa.astype(np.float64), requires_grad=True)
+    st = torch.tensor(isl.source.astype(np.float64), requires_grad=True)
+    for _ in range(max(args.warmup, 1)):
+        sess.solve(isl.kappa, isl.source)
+    t0 = time.perf_counter()
+    phis, H, ck = AD.ramped_trajectory(sess, kt, st, ticks=ticks, ramp=2.0, checkpoint_every=8)
+    t_fwd = (time.perf_counter() - t0) * 1000.0
+    L = AD.calibration_loss(phis[-1], kt, isl.vtype, isl.dims, rcomp, pt)
+    t0 = time.perf_counter()
+    L.backward()
+    t_bwd = (time.perf_counter() - t0) * 1000.0
+    adj_stats = sess.last_stats
+    g = kt.grad.numpy()
+    phi_T = phis[-1].detach().numpy()
+
+    dev = torch.device("cuda")
+    rc_d, pt_d = rcomp.to(dev), pt.to(dev)
+
+    def loss_np(phv, kv):
+        with torch.no_grad():
+            return float(AD.calibration_loss(torch.tensor(phv, device=dev), torch.tensor(kv, device=dev), isl.vtype,
+                                             isl.dims, rc_d, pt_d))
+
+    vox = rng.choice(np.where(isl.vtype != 0)[0], args.fd_voxels, replace=False)
+    src_T = (isl.source.astype(np.float32) * np.float32(2.0))
+    t0 = time.perf_counter()
+    fd, kink = AD.finite_difference_kappa(sess, isl.kappa, src_T, phi_T, loss_np, vox)
+    t_fd = time.perf_counter() - t0
+    ok = ~kink
+    rel = np.abs(g[vox][ok] - fd[ok]) / np.maximum(np.abs(fd[ok]), 1e-300)
+    line = {
+        "metric": "config-4 adjoint: max rel. error of dL/dkappa vs central FD (non-kink voxels)",
+        "value": float(rel.max()) if rel.size else None, "unit": "relative", "higher_is_better": False,
+        "n_gpus": 1, "data": "synthetic", "dtype": "f32",
+        "config": {"workload": "one 128x128x64 noise island (60 % occupancy, anchored component), 32 ticks, "
+                               "load ramped 1x->2x, checkpoint every 8 ticks",
+                   "active_voxels": int(isl.n_active), "precision": args.precision, "tol": 1e-10},
+        "median_rel_error": float(np.median(rel)) if rel.size else None,
+        "fd_voxels": int(len(vox)), "kink_hits": int(kink.sum()), "fd_step": 2.0 ** -10,
+        "forward_ms_per_tick": t_fwd / ticks, "backward_ms": t_bwd,
+        "adjoint_device_ms": float(adj_stats.device_ms), "recomputes": sess.recomputes,
+        "loss": float(L.detach()), "fd_seconds": t_fd,
+        "fp64_oracle_gradient": "checked at small sizes by tests/test_gpu_adjoint.py (a CPU FP64 solve of this "
+                                "island takes tens of minutes)",
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

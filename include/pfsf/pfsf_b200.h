@@ -86,6 +86,38 @@ PFSF_API pfsf_result pfsf_solve_to_tolerance(pfsf_engine engine, const int32_t* 
 PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine engine, int32_t island_id, double* out, int64_t capacity,
                                           int64_t* out_count);
 
+/* No counterpart in the reference ABI (which has no gradient code).
+ * Caller-owned host arrays of one island for the adjoint of the tolerance
+ * solve: grad_phi = dL/dphi in, grad_source = dL/ds and grad_kappa = dL/dkappa
+ * out (float32 x N each). */
+typedef struct pfsf_island_adjoint_buffers {
+    const void* grad_phi_addr;
+    int64_t grad_phi_bytes;
+    void* grad_source_addr;
+    int64_t grad_source_bytes;
+    void* grad_kappa_addr;
+    int64_t grad_kappa_bytes;
+} pfsf_island_adjoint_buffers;
+
+PFSF_API pfsf_result pfsf_register_island_adjoint(pfsf_engine engine, int32_t island_id,
+                                                  const pfsf_island_adjoint_buffers* bufs);
+
+/* Gradient of a loss L(phi) through the last pfsf_solve_to_tolerance of the
+ * same island set (same ids, same order): one solve A lambda = dL/dphi with
+ * the same symmetric operator, solver and precision mode (to rel_tol), then
+ * an edge-product pass
+ *     dL/ds_i     = lambda_i                                     (solid i)
+ *     dL/dkappa_i = - sum_j dw_ij/dk_i (lambda_i - lambda_j)(phi_i - phi_j)
+ * in FP64 from the FP64 forward solution, written to the registered
+ * grad_source / grad_kappa arrays (0 on air; dL/ds 0 on anchors).  The
+ * forward solution stays readable through pfsf_read_solution64.  Returns
+ * PFSF_ERROR_INVALID_ARG if an island has no adjoint buffers or the arena
+ * does not hold a forward solution of exactly this island set.  flags:
+ * PFSF_SOLVE_NO_READBACK leaves the gradients on the device. */
+PFSF_API pfsf_result pfsf_adjoint_to_tolerance(pfsf_engine engine, const int32_t* island_ids, int32_t count,
+                                               double rel_tol, int32_t max_iter, uint32_t flags,
+                                               pfsf_solve_stats* out);
+
 /* Diagnostic read of the per-island tick state (not part of the reference
  * ABI; used by parity tests and tooling).  field: 0 phi (float32 x N),
  * 1 history H (float32 x N), 2 damage d (float32 x N), 3 failure flags

@@ -239,3 +239,117 @@ def kappa_solve64(dims, kappa, vtype, source, tol=1e-12, maxit=20000, x0=None):
 def kappa_relres(dims, kappa, vtype, source, phi32):
     return lib().o_kappa_relres(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(source, np.float64),
                                 _c(phi32, np.float32))
+
+
+# ------------------------------------------------------- adjoint (FP64, numpy)
+# The reference has no gradient code; these restate the calculus of the
+# kappa operator above in FP64 so the device adjoint and the torch tooling
+# can be checked against it (and it against finite differences).
+
+def _dirs13():
+    """The 13 link directions counted once: offsets (dx, dy, dz) after the
+    centre in z-major order, with the operator's group scale c."""
+    out = []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                if (dz, dy, dx) > (0, 0, 0):
+                    m = abs(dx) + abs(dy) + abs(dz)
+                    out.append((dx, dy, dz, {1: 1.0, 2: 0.5, 3: 1.0 / 6.0}[m]))
+    return out
+
+
+def _pair_slices(d, n):
+    if d == 0:
+        return slice(0, n), slice(0, n)
+    if d == 1:
+        return slice(0, n - 1), slice(1, n)
+    return slice(1, n), slice(0, n - 1)
+
+
+def _links(dims):
+    """(si, sj, c) per direction: 3-D slices of the voxels i and their
+    neighbours j = i + offset, arrays shaped (lz, ly, lx)."""
+    lx, ly, lz = dims
+    for dx, dy, dz, c in _dirs13():
+        zi, zj = _pair_slices(dz, lz)
+        yi, yj = _pair_slices(dy, ly)
+        xi, xj = _pair_slices(dx, lx)
+        yield (zi, yi, xi), (zj, yj, xj), c
+
+
+def _grid(a, dims):
+    lx, ly, lz = dims
+    return np.asarray(a, np.float64).reshape(lz, ly, lx)
+
+
+def kappa_edge_product(dims, kappa, vtype, phi, lam):
+    """-sum_j dw_ij/dk_i (lam_i - lam_j)(phi_i - phi_j) per voxel (FP64);
+    lam = phi = 0 off the solid voxels; 0 on air."""
+    k = _grid(kappa, dims)
+    t = np.asarray(vtype).reshape(k.shape)
+    solid = t == 1
+    P = np.where(solid, _grid(phi, dims), 0.0)
+    Lm = np.where(solid, _grid(lam, dims), 0.0)
+    g = np.zeros_like(k)
+    for si, sj, c in _links(dims):
+        ki, kj = k[si], k[sj]
+        both = (t[si] != 0) & (t[sj] != 0) & ((ki + kj) > 0)
+        s = np.where(both, ki + kj, 1.0)
+        prod = (Lm[si] - Lm[sj]) * (P[si] - P[sj])
+        g[si] -= np.where(both, 2.0 * c * kj * kj / (s * s) * prod, 0.0)
+        g[sj] -= np.where(both, 2.0 * c * ki * ki / (s * s) * prod, 0.0)
+    g[t == 0] = 0.0
+    return g.reshape(-1)
+
+
+def kappa_adjoint64(dims, kappa, vtype, phi, grad_phi, tol=1e-13):
+    """dL/ds, dL/dkappa for dL/dphi = grad_phi through A(kappa) phi = s:
+    lambda = A^-1 grad_phi (A symmetric), dL/ds = lambda on solid voxels,
+    dL/dkappa = the edge product."""
+    g = np.where(np.asarray(vtype) == 1, np.asarray(grad_phi, np.float64), 0.0)
+    lam, _, rr = kappa_solve64(dims, np.asarray(kappa, np.float64), vtype, g, tol=tol, maxit=400000)
+    gs = np.where(np.asarray(vtype) == 1, lam, 0.0)
+    return gs, kappa_edge_product(dims, kappa, vtype, phi, lam), rr
+
+
+def flux_loss64(dims, kappa, vtype, phi, rcomp, phi_target):
+    """L = sum_solid softplus(flux_in_i / rcomp_i - 1) + 1/2 sum_solid (phi_i - phi_target_i)^2
+    with flux_in_i = sum_j w_ij max(phi_j - phi_i, 0) over the operator's links
+    (the failure scan's compressive inflow, SH/failure_scan.comp.glsl:89-158,
+    on the kappa link weights).  Returns (L, dL/dphi, direct dL/dkappa)."""
+    k = _grid(kappa, dims)
+    t = np.asarray(vtype).reshape(k.shape)
+    solid = t == 1
+    P = np.where(solid, _grid(phi, dims), 0.0)
+    rc = _grid(rcomp, dims)
+    links = []
+    flux = np.zeros_like(k)
+    for si, sj, c in _links(dims):
+        ki, kj = k[si], k[sj]
+        both = (t[si] != 0) & (t[sj] != 0) & ((ki + kj) > 0)
+        s = np.where(both, ki + kj, 1.0)
+        w = np.where(both, 2.0 * c * ki * kj / s, 0.0)
+        u = P[sj] - P[si]
+        flux[si] += w * np.maximum(u, 0.0)
+        flux[sj] += w * np.maximum(-u, 0.0)
+        links.append((si, sj, c, w, u, s, both))
+    z = np.where(solid, flux / np.where(solid, rc, 1.0) - 1.0, 0.0)
+    sp = np.logaddexp(0.0, z)
+    d = np.where(solid, P - _grid(phi_target, dims), 0.0)
+    L = float(np.sum(np.where(solid, sp, 0.0)) + 0.5 * np.sum(d * d))
+    a = np.where(solid, 1.0 / (1.0 + np.exp(-z)) / np.where(solid, rc, 1.0), 0.0)  # dL/dflux
+    gphi = d.copy()
+    gk = np.zeros_like(k)
+    for si, sj, c, w, u, s, both in links:
+        pos, neg = u > 0, u < 0
+        ai, aj = a[si], a[sj]
+        gphi[sj] += np.where(pos, ai * w, 0.0) - np.where(neg, aj * w, 0.0)
+        gphi[si] += np.where(neg, aj * w, 0.0) - np.where(pos, ai * w, 0.0)
+        dLdw = ai * np.maximum(u, 0.0) + aj * np.maximum(-u, 0.0)
+        ki, kj = k[si], k[sj]
+        gk[si] += np.where(both, 2.0 * c * kj * kj / (s * s) * dLdw, 0.0)
+        gk[sj] += np.where(both, 2.0 * c * ki * ki / (s * s) * dLdw, 0.0)
+    gphi[~solid] = 0.0
+    gk[t == 0] = 0.0
+    return L, gphi.reshape(-1), gk.reshape(-1)

@@ -19,6 +19,9 @@ struct Engine::Arena {
     float* hscratch = nullptr;       // pinned host scalars (plain mode)
     float* phi_out = nullptr;        // FP32 solution staging (device), aliases e
     std::vector<void*> pinned;       // host ranges registered for fast copies
+    bool solved = false;             // x64 holds a forward solution of this island set
+    bool b_stale = false;            // b holds an adjoint right-hand side, not the sources
+    double* xf = nullptr;            // adjoint: FP64 copy of the forward solution (own allocation)
 };
 
 }  // namespace pfsf_b200

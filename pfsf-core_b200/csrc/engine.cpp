@@ -40,6 +40,7 @@ inline int64_t rtz_limit(int64_t n) {
 Engine::Engine(const pfsf_config& cfg) : cfg_(cfg) {
     if (const char* f = std::getenv("PFSF_FAULT_ALLOC_AFTER")) fault_alloc_after_ = std::atoll(f);
     if (const char* f = std::getenv("PFSF_CLUSTER_MIN_VOXELS")) cluster_min_voxels_ = std::atoll(f);
+    if (const char* f = std::getenv("PFSF_GRID_MIN_VOXELS")) grid_min_voxels_ = std::atoll(f);
     if (const char* f = std::getenv("PFSF_CLUSTER")) cluster_size_ = std::atoi(f);
     if (const char* f = std::getenv("PFSF_WARP_MAX_VOXELS")) warp_max_voxels_ = std::atoll(f);
     if (const char* f = std::getenv("PFSF_SMOOTHER")) smoother_ = std::atoi(f);

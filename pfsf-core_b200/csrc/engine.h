@@ -9,6 +9,7 @@
 #include <utility>
 #include <vector>
 
+#include "kappa.h"
 #include "pfsf/pfsf.h"
 
 namespace pfsf_b200 {
@@ -54,6 +55,11 @@ struct HostBuffers {
     void* k_source = nullptr;
     void* k_kappa = nullptr;
     void* k_type = nullptr;
+    // adjoint buffers (pfsf_register_island_adjoint)
+    bool adjoint_registered = false;
+    const void* a_grad_phi = nullptr;
+    void* a_grad_source = nullptr;
+    void* a_grad_kappa = nullptr;
 };
 
 // Small device-side per-island tick result, read back in one copy.
@@ -145,6 +151,9 @@ public:
     pfsf_result solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter, uint32_t flags,
                                    pfsf_solve_stats* out);
     pfsf_result read_solution64(int32_t id, double* out, int64_t cap, int64_t* count);
+    pfsf_result register_adjoint(int32_t id, const pfsf_island_adjoint_buffers* b);
+    pfsf_result adjoint_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
+                                     uint32_t flags, pfsf_solve_stats* out);
     pfsf_result debug_read_field(int32_t id, int32_t field, void* out, int64_t bytes, int64_t* out_bytes);
 
     cudaStream_t stream() const { return stream_; }
@@ -161,6 +170,11 @@ private:
     bool ensure_compat(Island& isl);
     bool build_arena(const std::vector<Island*>& set);
     void free_arena();
+    bool collect_kappa_set(const int32_t* ids, int32_t count, std::vector<Island*>& set);
+    KArena solve_params(double tol, int32_t max_iter) const;
+    pfsf_result run_solve(const KArena& k, std::vector<KDesc>& res, int64_t& launches);
+    bool grid_barrier_failed() const;
+    void fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_solve_stats& st) const;
     bool upload(Island& isl);
     bool ensure_mg(Island& isl);
     bool ensure_pcg(Island& isl);
@@ -195,6 +209,7 @@ private:
     struct Arena;
     std::unique_ptr<Arena> arena_;
     int num_sms_ = 148;
+    int64_t grid_min_voxels_ = 1 << 21;    // PFSF_GRID_MIN_VOXELS: whole-GPU tier
     int64_t cluster_min_voxels_ = 131072;  // PFSF_CLUSTER_MIN_VOXELS
     int cluster_size_ = 16;               // PFSF_CLUSTER (16, 8 or 1)
     int64_t warp_max_voxels_ = 0;         // PFSF_WARP_MAX_VOXELS (0: no warp tier)

@@ -74,11 +74,13 @@ struct KappaState {
 namespace kappa {
 // Plans levels for an island (host).
 int plan_levels(int lx, int ly, int lz, KLevel* lev);
-// Batched solve: one persistent launch over all islands in the arena; the
-// first nbig islands of a.order are solved by thread-block clusters of
-// `cluster` CTAs (16, 8 or 1), the last nsmall by single warps, the rest by
-// single CTAs.  Returns 0 on success.
-int launch_batched(cudaStream_t s, const KArena& a, int nbig, int nsmall, int cluster, int num_sms);
+// Batched solve over all islands in the arena: the first ngiant islands of
+// a.order are solved one at a time by a cooperative launch of the whole GPU,
+// the next nbig by thread-block clusters of `cluster` CTAs (16, 8 or 1) in
+// one persistent launch, the last nsmall by single warps, the rest by single
+// CTAs.  a.queue[0..15] must be zero.  Returns 0 on success; a timed-out
+// grid barrier is reported later through a.queue[10] != 0.
+int launch_batched(cudaStream_t s, const KArena& a, int ngiant, int nbig, int nsmall, int cluster, int num_sms);
 // Prepare kernels: sanitise kappa, round to 16-bit, zero non-solid source.
 void launch_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total, const int64_t* dummy);
 // Per-island plain solve driven from the host (one kernel per operation).
@@ -86,6 +88,12 @@ void launch_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total, const 
 int64_t solve_plain(cudaStream_t s, const KArena& a, int isl, const KDesc& hdesc, KDesc* hres);
 int batched_threads();
 int64_t plain_scratch_floats();
+// Adjoint: b = g on solid voxels, x64 = 0 (kappa_adjoint.cu).
+void launch_adjoint_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total);
+// dL/dkappa -> gk, dL/ds -> gs for every arena voxel, from the forward
+// solution phi (FP64) and the adjoint solution in a.x64.
+void launch_edge_product(cudaStream_t s, const KArena& a, const double* phi, int64_t nfine_total, float* gk,
+                         float* gs, int num_sms);
 }  // namespace kappa
 
 }  // namespace pfsf_b200

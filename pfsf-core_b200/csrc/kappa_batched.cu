@@ -1,15 +1,19 @@
 // Batched tolerance solve: one persistent launch solves every island.
 //
-// Work distribution.  Islands are ordered largest first.  The kernel is
-// launched with thread-block clusters of C CTAs (C = 1 disables the cluster
-// phase).  Phase 1: each cluster takes the next "big" island from a queue
-// and its C CTAs solve it together -- cluster barriers (barrier.cluster,
-// release/acquire at cluster scope) between dependent passes, inner products
-// reduced across the cluster through distributed shared memory.  Phase 2:
-// when the big queue is empty every CTA independently takes small islands
-// from a second queue and solves each with CTA barriers only.  No grid-wide
-// synchronisation exists anywhere, so there is nothing to wait on across
-// clusters, and every island carries its own convergence state.
+// Work distribution.  Islands are ordered largest first.  Giant islands
+// (PFSF_GRID_MIN_VOXELS and up) are solved first, one at a time, by a
+// cooperative launch of the whole GPU (k_grid: a software grid barrier with a
+// bounded wait between dependent passes).  The rest go to k_batched, launched
+// with thread-block clusters of C CTAs (C = 1 disables the cluster phase).
+// Phase 1: each cluster takes the next "big" island from a queue and its C
+// CTAs solve it together -- cluster barriers (barrier.cluster, release/acquire
+// at cluster scope) between dependent passes, inner products reduced across
+// the cluster through distributed shared memory.  Phase 2: when the big queue
+// is empty every CTA independently takes islands from a second queue and
+// solves each with CTA barriers only; phase 3 does the same per warp for the
+// smallest islands.  k_batched has no grid-wide synchronisation, so there is
+// nothing to wait on across clusters, and every island carries its own
+// convergence state.
 //
 // Each island's solve: Galerkin hierarchy build, then outer FP64 refinement
 // around an inner FP32 PCG preconditioned by one V-cycle (see kappa_ops.cuh).
@@ -103,6 +107,78 @@ struct ClusterTeam {
     }
     __device__ double sum(double v) { return xsum<double>(v, sh->shd, sh->slotd); }
     __device__ float sum(float v) { return xsum<float>(v, sh->shf, sh->slotf); }
+};
+
+// Team = the whole grid (giant islands, one at a time).  The kernel is
+// launched cooperatively, so every CTA is resident; the barrier is a
+// generation barrier on two global words with a bounded wait: a CTA that
+// waits longer than kGridSpinLimit polls (about a second) sets the error
+// word and stops waiting, after which every later barrier returns at once and
+// the solve runs out its bounded iteration counts; the host reports the
+// error.  Inner products: CTA partials in a global double-buffered slot array,
+// summed in block order by every CTA (deterministic, identical everywhere).
+constexpr unsigned kGridSpinLimit = 1u << 22;
+constexpr int kGridMaxBlocks = 1024;
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+struct GridTeam {
+    SharedScratch* sh;
+    unsigned* count;  // arrivals at the current barrier
+    unsigned* gen;    // barrier generation
+    int* err;         // set on a timed-out wait
+    double* slots;    // [2][kGridMaxBlocks] CTA partials
+    int parity = 0;
+    __device__ int64_t t() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ int64_t T() const { return (int64_t)gridDim.x * blockDim.x; }
+    __device__ bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+    __device__ bool leader_warp() const { return blockIdx.x == 0 && threadIdx.x < 32; }
+    __device__ void sync() const {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned g = ld_acquire_gpu(gen);
+            __threadfence();
+            if (atomicAdd(count, 1u) == gridDim.x - 1) {
+                atomicExch(count, 0u);
+                __threadfence();
+                atomicAdd(gen, 1u);
+            } else {
+                unsigned spins = 0;
+                while (ld_acquire_gpu(gen) == g) {
+                    if (*(volatile int*)err) break;
+                    if (++spins > kGridSpinLimit) {
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+    }
+    template <class R>
+    __device__ R gsum(R v, R* local) {
+        const R part = cta_sum(v, local);
+        double* s = slots + parity * kGridMaxBlocks;
+        if (threadIdx.x == 0) s[blockIdx.x] = (double)part;
+        sync();
+        if (threadIdx.x < 32) {
+            double a = 0.0;
+            for (unsigned k = threadIdx.x; k < gridDim.x; k += 32) a += __ldcg(s + k);
+            a = warp_sum(a);
+            if (threadIdx.x == 0) local[33] = (R)a;
+        }
+        __syncthreads();
+        parity ^= 1;
+        return local[33];
+    }
+    __device__ double sum(double v) { return gsum<double>(v, sh->shd); }
+    __device__ float sum(float v) { return gsum<float>(v, sh->shf); }
 };
 
 // One V-cycle z = M r.  Levels above kWarpTailCells cells are processed by
@@ -301,10 +377,29 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
     }
 }
 
-// queue[0]: big islands taken by clusters; queue[1]: small islands taken by CTAs.
+// Giant islands (a.order[0 .. ngiant)): the whole grid solves them one after
+// another.  Barrier words and partial slots live in the arena's queue and
+// scratch regions (zeroed by the host before the launch).
+template <int P>
+__global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
+    k_grid(const __grid_constant__ KArena A, int ngiant) {
+    __shared__ SharedScratch sh;
+    GridTeam tm{&sh, reinterpret_cast<unsigned*>(A.queue + 8), reinterpret_cast<unsigned*>(A.queue + 9), A.queue + 10,
+                reinterpret_cast<double*>(A.scratch)};
+    for (int q = 0; q < ngiant; q++) {
+        KDesc& D = A.desc[A.order[q]];
+        if (A.fp64_dots) team_solve<P, double>(A, D, tm);
+        else team_solve<P, float>(A, D, tm);
+        tm.sync();
+    }
+}
+
+// Islands a.order[base ..): queue[0] hands the next nbig ones to clusters,
+// queue[1] the following ones to single CTAs, queue[2] the last nsmall ones
+// to single warps.
 template <int P, int C>
 __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
-    k_batched(const __grid_constant__ KArena A, int nbig, int nsmall) {
+    k_batched(const __grid_constant__ KArena A, int base, int nbig, int nsmall) {
     __shared__ SharedScratch sh;
     if constexpr (C > 1) {
         cg::cluster_group cl = cg::this_cluster();
@@ -312,9 +407,9 @@ __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
         for (;;) {
             if (cl.block_rank() == 0 && threadIdx.x == 0) sh.next = atomicAdd(&A.queue[0], 1);
             cl.sync();
-            const int q = *cl.map_shared_rank(&sh.next, 0);
-            if (q >= nbig) break;
-            KDesc& D = A.desc[A.order[q]];
+            const int k = *cl.map_shared_rank(&sh.next, 0);
+            if (k >= nbig) break;
+            KDesc& D = A.desc[A.order[base + k]];
             if (A.fp64_dots) team_solve<P, double>(A, D, tm);
             else team_solve<P, float>(A, D, tm);
             cl.sync();
@@ -326,7 +421,7 @@ __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
     for (;;) {
         if (threadIdx.x == 0) sh.next = atomicAdd(&A.queue[1], 1);
         __syncthreads();
-        const int q = nbig + sh.next;
+        const int q = base + nbig + sh.next;
         __syncthreads();
         if (q >= nmid_end) break;
         KDesc& D = A.desc[A.order[q]];
@@ -349,8 +444,30 @@ __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
     }
 }
 
+// Cooperative launch of k_grid: one resident grid of per_sm CTAs per SM.
+template <int P>
+cudaError_t launch_grid(cudaStream_t s, const KArena& a, int ngiant, int num_sms) {
+    auto kern = k_grid<P>;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, 0) != cudaSuccess ||
+        per_sm <= 0)
+        return cudaErrorInvalidConfiguration;
+    const int ctas = std::min(num_sms * per_sm, kGridMaxBlocks);
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(kBatchedThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a, ngiant);
+}
+
 template <int P, int C>
-cudaError_t launch_one(cudaStream_t s, const KArena& a, int nbig, int nsmall, int num_sms) {
+cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int nsmall, int num_sms) {
     auto kern = k_batched<P, C>;
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
@@ -383,35 +500,42 @@ cudaError_t launch_one(cudaStream_t s, const KArena& a, int nbig, int nsmall, in
         cfg.attrs = nullptr;
         cfg.numAttrs = 0;
     }
-    cfg.gridDim = dim3(std::max(C, std::min(ctas, std::max(C, a.nisl * C))));
-    return cudaLaunchKernelEx(&cfg, kern, a, nbig, nsmall);
+    const int rest = std::max(1, a.nisl - base);
+    cfg.gridDim = dim3(std::max(C, std::min(ctas, std::max(C, rest * C))));
+    return cudaLaunchKernelEx(&cfg, kern, a, base, nbig, nsmall);
 }
 
 template <int P>
-cudaError_t launch_p(cudaStream_t s, const KArena& a, int nbig, int nsmall, int cluster, int num_sms) {
+cudaError_t launch_p(cudaStream_t s, const KArena& a, int ngiant, int nbig, int nsmall, int cluster, int num_sms) {
+    if (ngiant > 0) {
+        const cudaError_t e = launch_grid<P>(s, a, ngiant, num_sms);
+        if (e != cudaSuccess) return e;
+        if (ngiant >= a.nisl) return cudaSuccess;
+    }
     if (nbig > 0 && cluster >= 16) {
-        if (launch_one<P, 16>(s, a, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
+        if (launch_one<P, 16>(s, a, ngiant, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
         cudaGetLastError();
     }
     if (nbig > 0 && cluster >= 8) {
-        if (launch_one<P, 8>(s, a, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
+        if (launch_one<P, 8>(s, a, ngiant, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
         cudaGetLastError();
     }
-    return launch_one<P, 1>(s, a, 0, nsmall, num_sms);
+    return launch_one<P, 1>(s, a, ngiant, 0, nsmall, num_sms);
 }
 
 }  // namespace
 
 int batched_threads() { return kBatchedThreads; }
 
-// nbig: number of leading islands (in a.order) solved by whole clusters;
-// nsmall: number of trailing islands solved by single warps.
-int launch_batched(cudaStream_t s, const KArena& a, int nbig, int nsmall, int cluster, int num_sms) {
+// ngiant: leading islands (in a.order) solved by the whole grid; nbig: the
+// next ones, solved by whole clusters; nsmall: trailing islands solved by
+// single warps.
+int launch_batched(cudaStream_t s, const KArena& a, int ngiant, int nbig, int nsmall, int cluster, int num_sms) {
     cudaError_t e;
     switch (a.prec) {
-        case 1: e = launch_p<1>(s, a, nbig, nsmall, cluster, num_sms); break;
-        case 2: e = launch_p<2>(s, a, nbig, nsmall, cluster, num_sms); break;
-        default: e = launch_p<0>(s, a, nbig, nsmall, cluster, num_sms); break;
+        case 1: e = launch_p<1>(s, a, ngiant, nbig, nsmall, cluster, num_sms); break;
+        case 2: e = launch_p<2>(s, a, ngiant, nbig, nsmall, cluster, num_sms); break;
+        default: e = launch_p<0>(s, a, ngiant, nbig, nsmall, cluster, num_sms); break;
     }
     if (e != cudaSuccess) {
         std::fprintf(stderr, "[libpfsf] batched solve launch failed: %s\n", cudaGetErrorString(e));

@@ -96,9 +96,10 @@ void Engine::free_arena() {
     for (void* h : arena_->pinned) cudaHostUnregister(h);
     if (arena_->base) cudaFree(arena_->base);
     if (arena_->hscratch) cudaFreeHost(arena_->hscratch);
+    if (arena_->xf) cudaFree(arena_->xf);
     {
         std::lock_guard<std::mutex> lk(stats_mtx_);
-        vram_used_ -= (int64_t)arena_->bytes;
+        vram_used_ -= (int64_t)arena_->bytes + (arena_->xf ? arena_->nfine * 8 : 0);
     }
     arena_.reset();
 }
@@ -202,32 +203,18 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     return true;
 }
 
-pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
-                                       uint32_t flags, pfsf_solve_stats* out) {
-    if (!available_) return PFSF_ERROR_NOT_INIT;
-    if (count < 0 || (count > 0 && !ids) || !(tol > 0.0)) return PFSF_ERROR_INVALID_ARG;
-    std::vector<Island*> set;
+bool Engine::collect_kappa_set(const int32_t* ids, int32_t count, std::vector<Island*>& set) {
+    set.clear();
     for (int32_t k = 0; k < count; k++) {
         Island* s = find(ids[k]);
-        if (!s || !s->hosts.kappa_registered) return PFSF_ERROR_INVALID_ARG;
+        if (!s || !s->hosts.kappa_registered) return false;
         if (std::find(set.begin(), set.end(), s) == set.end()) set.push_back(s);
     }
-    pfsf_solve_stats st{};
-    st.struct_bytes = (int32_t)sizeof(pfsf_solve_stats);
-    if (set.empty()) {
-        if (out) *out = st;
-        return PFSF_OK;
-    }
-    bool same = arena_ && arena_->prec == (int)precision_ && arena_->ids.size() == set.size();
-    if (same)
-        for (size_t k = 0; k < set.size(); k++) same &= arena_->ids[k] == set[k]->id;
-    bool do_upload = !(flags & PFSF_SOLVE_NO_UPLOAD);
-    if (!same) {
-        if (!build_arena(set)) return PFSF_ERROR_OUT_OF_VRAM;
-        do_upload = true;
-    }
-    Arena& A = *arena_;
-    KArena k = A.dev;
+    return true;
+}
+
+KArena Engine::solve_params(double tol, int32_t max_iter) const {
+    KArena k = arena_->dev;
     k.tol = tol;
     k.eta_min = 1e-4;
     k.max_outer = 8;
@@ -254,6 +241,95 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
             rho = rn;
         }
     }
+    return k;
+}
+
+// Launches the solve of every island in the arena (x64 is the starting
+// guess, b the right-hand side) and queues the copy of the per-island
+// results into res (valid after the stream is synchronised).
+pfsf_result Engine::run_solve(const KArena& k, std::vector<KDesc>& res, int64_t& nl) {
+    Arena& A = *arena_;
+    res.resize(A.desc.size());
+    nl = 0;
+    if (solve_mode_ == PFSF_SOLVE_BATCHED) {
+        cudaMemsetAsync(k.queue, 0, 16 * sizeof(int), stream_);
+        // islands at or above the grid threshold are solved by the whole GPU
+        // (one at a time), those at or above the cluster threshold by whole
+        // thread-block clusters (largest first), islands below the warp
+        // threshold by single warps, the rest by single CTAs
+        int ngiant = 0, nbig = 0, nsmall = 0;
+        for (const KDesc& d : A.desc) {
+            ngiant += d.n >= grid_min_voxels_ ? 1 : 0;
+            nbig += (d.n >= cluster_min_voxels_ && d.n < grid_min_voxels_) ? 1 : 0;
+            nsmall += d.n < warp_max_voxels_ ? 1 : 0;
+        }
+        if (kappa::launch_batched(stream_, k, ngiant, nbig, nsmall, cluster_size_, num_sms_) != 0)
+            return PFSF_ERROR_VULKAN;
+        nl = (ngiant > 0 ? 1 : 0) + (ngiant < (int)A.desc.size() ? 1 : 0);
+        int* flag = reinterpret_cast<int*>(A.hscratch) + 48;
+        *flag = 0;
+        cudaMemcpyAsync(flag, k.queue + 10, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+    } else {
+        for (size_t q = 0; q < A.desc.size(); q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &res[q]);
+    }
+    launches_ += nl;
+    cudaMemcpyAsync(res.data(), k.desc, sizeof(KDesc) * res.size(), cudaMemcpyDeviceToHost, stream_);
+    return PFSF_OK;
+}
+
+// After the stream is synchronised: did a whole-GPU barrier time out?
+bool Engine::grid_barrier_failed() const {
+    return solve_mode_ == PFSF_SOLVE_BATCHED && arena_ && reinterpret_cast<const int*>(arena_->hscratch)[48] != 0;
+}
+
+void Engine::fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_solve_stats& st) const {
+    const Arena& A = *arena_;
+    st.islands_solved = (int32_t)res.size();
+    for (size_t q = 0; q < res.size(); q++) {
+        const KDesc& d = res[q];
+        st.islands_converged += d.converged ? 1 : 0;
+        st.max_iterations = std::max(st.max_iterations, d.inner_iters);
+        st.max_rel_residual = std::max(st.max_rel_residual, d.relres);
+        st.inner_iterations_total += d.inner_iters;
+        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps, k.smoother, k.cheb_k);
+        st.active_voxels += A.active[q];
+    }
+    if (solve_mode_ == PFSF_SOLVE_BATCHED) {
+        unsigned long long t0 = ~0ull, t1 = 0;
+        for (const KDesc& d : res) {
+            t0 = std::min(t0, d.t_start);
+            t1 = std::max(t1, d.t_end);
+            const double ms = (double)(d.t_end - d.t_start) * 1e-6;
+            st.island_ms_sum += ms;
+            st.island_ms_max = std::max(st.island_ms_max, ms);
+        }
+        st.span_ms = t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
+    }
+}
+
+pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
+                                       uint32_t flags, pfsf_solve_stats* out) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (count < 0 || (count > 0 && !ids) || !(tol > 0.0)) return PFSF_ERROR_INVALID_ARG;
+    std::vector<Island*> set;
+    if (!collect_kappa_set(ids, count, set)) return PFSF_ERROR_INVALID_ARG;
+    pfsf_solve_stats st{};
+    st.struct_bytes = (int32_t)sizeof(pfsf_solve_stats);
+    if (set.empty()) {
+        if (out) *out = st;
+        return PFSF_OK;
+    }
+    bool same = arena_ && arena_->prec == (int)precision_ && arena_->ids.size() == set.size();
+    if (same)
+        for (size_t k = 0; k < set.size(); k++) same &= arena_->ids[k] == set[k]->id;
+    bool do_upload = !(flags & PFSF_SOLVE_NO_UPLOAD);
+    if (!same) {
+        if (!build_arena(set)) return PFSF_ERROR_OUT_OF_VRAM;
+        do_upload = true;
+    }
+    Arena& A = *arena_;
+    if (A.b_stale) do_upload = true;  // an adjoint solve replaced the sources
+    const KArena k = solve_params(tol, max_iter);
 
     cudaEvent_t ev[4];
     for (auto& e : ev) cudaEventCreate(&e);
@@ -275,28 +351,14 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
         }
         kappa::launch_prepare(stream_, k, A.nfine, nullptr);
         launches_++;
+        A.b_stale = false;
     }
     cudaEventRecord(ev[1], stream_);
     if (flags & PFSF_SOLVE_COLD_START) cudaMemsetAsync(k.x64, 0, (size_t)A.nfine * 8, stream_);
+    std::vector<KDesc> res;
     int64_t nl = 0;
-    std::vector<KDesc> res(set.size());
-    if (batched) {
-        cudaMemsetAsync(k.queue, 0, 4 * sizeof(int), stream_);
-        // islands at or above the cluster threshold are solved by whole
-        // thread-block clusters (largest first), islands below the warp
-        // threshold by single warps, the rest by single CTAs
-        int nbig = 0, nsmall = 0;
-        for (const KDesc& d : A.desc) {
-            nbig += d.n >= cluster_min_voxels_ ? 1 : 0;
-            nsmall += d.n < warp_max_voxels_ ? 1 : 0;
-        }
-        if (kappa::launch_batched(stream_, k, nbig, nsmall, cluster_size_, num_sms_) != 0) return PFSF_ERROR_VULKAN;
-        nl = 1;
-    } else {
-        for (size_t q = 0; q < set.size(); q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &res[q]);
-    }
+    if (pfsf_result rc = run_solve(k, res, nl); rc != PFSF_OK) return rc;
     cudaEventRecord(ev[2], stream_);
-    launches_ += nl;
     if (!(flags & PFSF_SOLVE_NO_READBACK)) {
         kappa::launch_to_f32(stream_, k, A.nfine);
         launches_++;
@@ -308,40 +370,111 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
                 return PFSF_ERROR_VULKAN;
         }
     }
-    cudaMemcpyAsync(res.data(), k.desc, sizeof(KDesc) * set.size(), cudaMemcpyDeviceToHost, stream_);
     cudaEventRecord(ev[3], stream_);
-    if (!CU_OK(cudaStreamSynchronize(stream_))) return PFSF_ERROR_VULKAN;
+    if (!CU_OK(cudaStreamSynchronize(stream_)) || grid_barrier_failed()) return PFSF_ERROR_VULKAN;
     float t_up = 0, t_solve = 0, t_rb = 0;
     cudaEventElapsedTime(&t_up, ev[0], ev[1]);
     cudaEventElapsedTime(&t_solve, ev[1], ev[2]);
     cudaEventElapsedTime(&t_rb, ev[2], ev[3]);
     for (auto& e : ev) cudaEventDestroy(e);
-    st.islands_solved = (int32_t)set.size();
-    for (size_t q = 0; q < res.size(); q++) {
-        const KDesc& d = res[q];
-        st.islands_converged += d.converged ? 1 : 0;
-        st.max_iterations = std::max(st.max_iterations, d.inner_iters);
-        st.max_rel_residual = std::max(st.max_rel_residual, d.relres);
-        st.inner_iterations_total += d.inner_iters;
-        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps, k.smoother, k.cheb_k);
-        st.active_voxels += A.active[q];
-    }
-    if (batched) {
-        unsigned long long t0 = ~0ull, t1 = 0;
-        for (const KDesc& d : res) {
-            t0 = std::min(t0, d.t_start);
-            t1 = std::max(t1, d.t_end);
-            const double ms = (double)(d.t_end - d.t_start) * 1e-6;
-            st.island_ms_sum += ms;
-            st.island_ms_max = std::max(st.island_ms_max, ms);
-        }
-        st.span_ms = t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
-    }
+    fill_stats(k, res, st);
     st.device_ms = t_solve;
     st.upload_ms = t_up;
     st.readback_ms = t_rb;
     st.kernel_launches = (int32_t)std::min<int64_t>(nl, INT32_MAX);
     A.desc = res;
+    A.solved = true;
+    if (out) *out = st;
+    return PFSF_OK;
+}
+
+pfsf_result Engine::register_adjoint(int32_t id, const pfsf_island_adjoint_buffers* b) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (!b || !b->grad_phi_addr || !b->grad_source_addr || !b->grad_kappa_addr) return PFSF_ERROR_INVALID_ARG;
+    Island* s = find(id);
+    if (!s) return PFSF_ERROR_INVALID_ARG;
+    const int64_t bytes = 4 * s->n;
+    if (b->grad_phi_bytes < bytes || b->grad_source_bytes < bytes || b->grad_kappa_bytes < bytes)
+        return PFSF_ERROR_INVALID_ARG;
+    HostBuffers& h = s->hosts;
+    h.a_grad_phi = b->grad_phi_addr;
+    h.a_grad_source = b->grad_source_addr;
+    h.a_grad_kappa = b->grad_kappa_addr;
+    h.adjoint_registered = true;
+    return PFSF_OK;
+}
+
+pfsf_result Engine::adjoint_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
+                                         uint32_t flags, pfsf_solve_stats* out) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (count <= 0 || !ids || !(tol > 0.0)) return PFSF_ERROR_INVALID_ARG;
+    std::vector<Island*> set;
+    if (!collect_kappa_set(ids, count, set)) return PFSF_ERROR_INVALID_ARG;
+    for (const Island* s : set)
+        if (!s->hosts.adjoint_registered) return PFSF_ERROR_INVALID_ARG;
+    // the arena must hold the forward solution of exactly this island set
+    if (!arena_ || !arena_->solved || arena_->prec != (int)precision_ || arena_->ids.size() != set.size())
+        return PFSF_ERROR_INVALID_ARG;
+    for (size_t q = 0; q < set.size(); q++)
+        if (arena_->ids[q] != set[q]->id) return PFSF_ERROR_INVALID_ARG;
+    Arena& A = *arena_;
+    if (!A.xf) {
+        if (!CU_OK(cudaMalloc(&A.xf, (size_t)A.nfine * 8))) {
+            cudaGetLastError();
+            A.xf = nullptr;
+            return PFSF_ERROR_OUT_OF_VRAM;
+        }
+        std::lock_guard<std::mutex> lk(stats_mtx_);
+        vram_used_ += A.nfine * 8;
+    }
+    const KArena k = solve_params(tol, max_iter);
+    pfsf_solve_stats st{};
+    st.struct_bytes = (int32_t)sizeof(pfsf_solve_stats);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[0], stream_);
+    // keep the forward solution; load dL/dphi as the right-hand side
+    bool ok = CU_OK(cudaMemcpyAsync(A.xf, k.x64, (size_t)A.nfine * 8, cudaMemcpyDeviceToDevice, stream_));
+    for (size_t q = 0; q < set.size() && ok; q++)
+        ok &= CU_OK(cudaMemcpyAsync(const_cast<float*>(k.b) + A.desc[q].off, set[q]->hosts.a_grad_phi,
+                                    (size_t)set[q]->n * 4, cudaMemcpyHostToDevice, stream_));
+    if (!ok) return PFSF_ERROR_VULKAN;
+    A.b_stale = true;
+    kappa::launch_adjoint_prepare(stream_, k, A.nfine);
+    launches_++;
+    cudaEventRecord(ev[1], stream_);
+    std::vector<KDesc> res;
+    int64_t nl = 0;
+    if (pfsf_result rc = run_solve(k, res, nl); rc != PFSF_OK) return rc;
+    // gradients into the (now free) r / z work vectors, then restore x64
+    kappa::launch_edge_product(stream_, k, A.xf, A.nfine, k.r, k.z, num_sms_);
+    launches_++;
+    nl++;
+    cudaEventRecord(ev[2], stream_);
+    if (!(flags & PFSF_SOLVE_NO_READBACK)) {
+        for (size_t q = 0; q < set.size() && ok; q++) {
+            const Island* s = set[q];
+            const int64_t o = A.desc[q].off;
+            ok &= CU_OK(cudaMemcpyAsync(s->hosts.a_grad_kappa, k.r + o, (size_t)s->n * 4, cudaMemcpyDeviceToHost,
+                                        stream_));
+            ok &= CU_OK(cudaMemcpyAsync(s->hosts.a_grad_source, k.z + o, (size_t)s->n * 4, cudaMemcpyDeviceToHost,
+                                        stream_));
+        }
+    }
+    ok &= CU_OK(cudaMemcpyAsync(k.x64, A.xf, (size_t)A.nfine * 8, cudaMemcpyDeviceToDevice, stream_));
+    cudaEventRecord(ev[3], stream_);
+    if (!ok || !CU_OK(cudaStreamSynchronize(stream_)) || grid_barrier_failed()) return PFSF_ERROR_VULKAN;
+    float t_up = 0, t_solve = 0, t_rb = 0;
+    cudaEventElapsedTime(&t_up, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_solve, ev[1], ev[2]);
+    cudaEventElapsedTime(&t_rb, ev[2], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    // the per-island results of the forward solve stay the arena's record
+    fill_stats(k, res, st);
+    st.device_ms = t_solve;
+    st.upload_ms = t_up;
+    st.readback_ms = t_rb;
+    st.kernel_launches = (int32_t)std::min<int64_t>(nl, INT32_MAX);
     if (out) *out = st;
     return PFSF_OK;
 }

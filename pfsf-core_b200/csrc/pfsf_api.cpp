@@ -173,6 +173,17 @@ PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine e, int32_t id, double* out
     return g ? g->read_solution64(id, out, cap, count) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_register_island_adjoint(pfsf_engine e, int32_t id, const pfsf_island_adjoint_buffers* b) {
+    Engine* g = E(e);
+    return g ? g->register_adjoint(id, b) : PFSF_ERROR_INVALID_ARG;
+}
+
+PFSF_API pfsf_result pfsf_adjoint_to_tolerance(pfsf_engine e, const int32_t* ids, int32_t count, double rel_tol,
+                                               int32_t max_iter, uint32_t flags, pfsf_solve_stats* out) {
+    Engine* g = E(e);
+    return g ? g->adjoint_to_tolerance(ids, count, rel_tol, max_iter, flags, out) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine e, int32_t id, int32_t field, void* out, int64_t bytes,
                                            int64_t* out_bytes) {
     Engine* g = E(e);

@@ -75,6 +75,11 @@ class KappaBuffers(C.Structure):
                 for n, t in ((pair + "_addr", C.c_void_p), (pair + "_bytes", C.c_int64))]
 
 
+class AdjointBuffers(C.Structure):
+    _fields_ = [(n, t) for pair in ["grad_phi", "grad_source", "grad_kappa"]
+                for n, t in ((pair + "_addr", C.c_void_p), (pair + "_bytes", C.c_int64))]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("struct_bytes", C.c_int32), ("islands_solved", C.c_int32), ("islands_converged", C.c_int32),
                 ("max_iterations", C.c_int32), ("max_rel_residual", C.c_double), ("device_ms", C.c_float),
@@ -126,6 +131,9 @@ def load():
         "pfsf_solve_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
                                      C.POINTER(SolveStats)], C.c_int),
         "pfsf_read_solution64": ([E, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_register_island_adjoint": ([E, C.c_int32, C.POINTER(AdjointBuffers)], C.c_int),
+        "pfsf_adjoint_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
+                                       C.POINTER(SolveStats)], C.c_int),
         "pfsf_debug_read_field": ([E, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
         "pfsf_compact_failures_noalloc": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, Pos, C.c_void_p, C.c_int32,
                                            C.c_void_p, C.c_void_p], C.c_int),
@@ -210,6 +218,23 @@ class Engine:
         st = SolveStats()
         rc = self.L.pfsf_solve_to_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, tol,
                                             max_iter, flags, C.byref(st))
+        return rc, st
+
+    def register_adjoint(self, iid, grad_phi, grad_source, grad_kappa):
+        arrs = [grad_phi, grad_source, grad_kappa]
+        for a in arrs:
+            assert a.dtype == np.float32 and a.flags.c_contiguous
+        b = AdjointBuffers(*[v for a in arrs for v in (_ptr(a), a.nbytes)])
+        self._keep[("a", iid)] = arrs
+        return self.L.pfsf_register_island_adjoint(self.h, iid, C.byref(b))
+
+    def adjoint(self, ids, tol=1e-6, max_iter=500, flags=0):
+        """dL/ds and dL/dkappa into the registered adjoint arrays, from the
+        registered dL/dphi, through the last solve of the same island set."""
+        ids = np.ascontiguousarray(ids, np.int32)
+        st = SolveStats()
+        rc = self.L.pfsf_adjoint_to_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, tol,
+                                              max_iter, flags, C.byref(st))
         return rc, st
 
     def read_solution64(self, iid, n):
