@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["batch", "single", "adjoint"], default="batch")
     ap.add_argument("--fd-voxels", type=int, default=256)
+    ap.add_argument("--dims", default="256,256,128", help="single workload: island sides x,y,z")
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="batch workload with N GPUs: every rank its own 4096 islands (weak) or one 4096-island "
+                         "workload partitioned by active voxels (strong)")
     ap.add_argument("--islands", type=int, default=4096)
     ap.add_argument("--target-active", type=float, default=6.0e7)
     ap.add_argument("--tol", type=float, default=1e-6)
@@ -71,8 +75,18 @@ def dist_info():
 def make_workload(args, rank):
     from pfsf_b200 import synth
     if args.workload == "single":
-        isl = synth.noise_island((256, 256, 128), seed=11 + rank)
+        isl = synth.noise_island(tuple(int(v) for v in args.dims.split(",")), seed=11 + rank)
         return [isl], {"grid_total": isl.n, "active_total": isl.n_active, "scale": 1.0}
+    if args.scaling == "strong":
+        # one workload, partitioned across the ranks by active voxels
+        from pfsf_b200 import shard
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        isls, meta = synth.batch(args.islands, seed=7, target_active=args.target_active,
+                                 workers=min(32, os.cpu_count() or 1))
+        mine = shard.plan_shards([i.n_active for i in isls], ws)[rank]
+        isls = [isls[i] for i in mine]
+        meta = dict(meta, grid_total=sum(i.n for i in isls), active_total=sum(i.n_active for i in isls))
+        return isls, meta
     return synth.batch(args.islands, seed=7 + 1000 * rank, target_active=args.target_active,
                        workers=min(32, os.cpu_count() or 1))
 
@@ -339,11 +353,12 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": "ms/tick", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": args.scaling,
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": ((f"{len(isls)} islands/GPU (log-uniform sides, scale {meta['scale']:.3f}), "
                                      if args.workload == "batch" else
-                                     "one 256x256x128 noise island (60 % occupancy, anchored component), ")
+                                     f"one {args.dims.replace(',', 'x')} noise island (60 % occupancy, anchored "
+                                     "component), ")
                                     + f"{meta['grid_total']} grid / {meta['active_total']} active voxels, "
                                     f"cold start, tol {args.tol:g}"),
                        "islands": len(isls), "grid_voxels": meta["grid_total"], "active_voxels": meta["active_total"],

@@ -22,7 +22,7 @@
 #include <algorithm>
 #include <cstdio>
 
-#include "kappa_ops.cuh"
+#include "kappa_march.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -52,6 +52,7 @@ struct SharedScratch {
 
 // Team = one CTA.
 struct CtaTeam {
+    static constexpr bool kMarch = false;  // fine passes by the generic per-voxel ops
     SharedScratch* sh;
     __device__ int64_t t() const { return threadIdx.x; }
     __device__ int64_t T() const { return blockDim.x; }
@@ -64,6 +65,7 @@ struct CtaTeam {
 
 // Team = one warp (small islands): warp barriers only, shuffle reductions.
 struct WarpTeam {
+    static constexpr bool kMarch = false;
     __device__ int64_t t() const { return threadIdx.x & 31; }
     __device__ int64_t T() const { return 32; }
     __device__ bool leader() const { return (threadIdx.x & 31) == 0; }
@@ -79,6 +81,7 @@ struct WarpTeam {
 // rank order by every CTA -- identical, deterministic results everywhere.
 template <int C>
 struct ClusterTeam {
+    static constexpr bool kMarch = false;
     SharedScratch* sh;
     int parity = 0;
     __device__ int64_t t() const { return (int64_t)cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
@@ -127,12 +130,16 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 }
 
 struct GridTeam {
+    static constexpr bool kMarch = true;  // fine passes by plane marching (kappa_march.cuh)
     SharedScratch* sh;
     unsigned* count;  // arrivals at the current barrier
     unsigned* gen;    // barrier generation
     int* err;         // set on a timed-out wait
     double* slots;    // [2][kGridMaxBlocks] CTA partials
+    MarchTile* mt;
     int parity = 0;
+    __device__ int cta() const { return blockIdx.x; }
+    __device__ int ncta() const { return gridDim.x; }
     __device__ int64_t t() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
     __device__ int64_t T() const { return (int64_t)gridDim.x * blockDim.x; }
     __device__ bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
@@ -180,6 +187,59 @@ struct GridTeam {
     __device__ double sum(double v) { return gsum<double>(v, sh->shd); }
     __device__ float sum(float v) { return gsum<float>(v, sh->shf); }
 };
+
+// Fine-level passes: plane marching / four-wide streaming for marching teams,
+// the generic per-voxel ops otherwise.
+template <class TeamT>
+__device__ __forceinline__ void t_outer_residual(const KArena& A, const KDesc& D, TeamT& tm, double& rr, double& bb) {
+    if constexpr (TeamT::kMarch) mop_outer_residual(A, D, *tm.mt, tm.cta(), tm.ncta(), rr, bb);
+    else op_outer_residual(A, D, (int)tm.t(), (int)tm.T(), rr, bb);
+}
+template <class R, class TeamT>
+__device__ __forceinline__ void t_matvec(const KArena& A, const KDesc& D, TeamT& tm, R& pq) {
+    if constexpr (TeamT::kMarch) mop_matvec(A, D, *tm.mt, tm.cta(), tm.ncta(), pq);
+    else op_matvec(A, D, (int)tm.t(), (int)tm.T(), pq);
+}
+template <class R, class TeamT>
+__device__ __forceinline__ void t_update(const KArena& A, const KDesc& D, TeamT& tm, float alpha, R& rr) {
+    if constexpr (TeamT::kMarch) vop_update(A, D, (int)tm.t(), (int)tm.T(), alpha, rr);
+    else op_update(A, D, (int)tm.t(), (int)tm.T(), alpha, rr);
+}
+template <class R, class TeamT>
+__device__ __forceinline__ void t_dot_rz(const KArena& A, const KDesc& D, TeamT& tm, R& rz) {
+    if constexpr (TeamT::kMarch) vop_dot_rz(A, D, (int)tm.t(), (int)tm.T(), rz);
+    else op_dot_rz(A, D, (int)tm.t(), (int)tm.T(), rz);
+}
+template <class TeamT>
+__device__ __forceinline__ void t_pupdate(const KArena& A, const KDesc& D, TeamT& tm, float beta) {
+    if constexpr (TeamT::kMarch) vop_pupdate(A, D, (int)tm.t(), (int)tm.T(), beta);
+    else op_pupdate(A, D, (int)tm.t(), (int)tm.T(), beta);
+}
+template <class TeamT>
+__device__ __forceinline__ void t_accumulate(const KArena& A, const KDesc& D, TeamT& tm) {
+    if constexpr (TeamT::kMarch) vop_accumulate(A, D, (int)tm.t(), (int)tm.T());
+    else op_accumulate(A, D, (int)tm.t(), (int)tm.T());
+}
+template <int P, class TeamT>
+__device__ __forceinline__ void t_restrict0(const KArena& A, const KDesc& D, TeamT& tm) {
+    if constexpr (TeamT::kMarch) mop_restrict0<P>(A, D, *tm.mt, tm.cta(), tm.ncta());
+    else op_restrict0<P>(A, D, (int)tm.t(), (int)tm.T());
+}
+template <class TeamT>
+__device__ __forceinline__ void t_cheb0_first(const KArena& A, const KDesc& D, TeamT& tm, float c2) {
+    if constexpr (TeamT::kMarch) vop_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2);
+    else op_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2);
+}
+template <int P, class TeamT>
+__device__ __forceinline__ void t_cheb0_d(const KArena& A, const KDesc& D, TeamT& tm, float c1, float c2) {
+    if constexpr (TeamT::kMarch) mop_cheb0_d<P>(A, D, *tm.mt, tm.cta(), tm.ncta(), c1, c2);
+    else op_cheb0_d<P>(A, D, (int)tm.t(), (int)tm.T(), c1, c2);
+}
+template <class TeamT>
+__device__ __forceinline__ void t_cheb0_z(const KArena& A, const KDesc& D, TeamT& tm) {
+    if constexpr (TeamT::kMarch) vop_cheb0_z(A, D, (int)tm.t(), (int)tm.T());
+    else op_cheb0_z(A, D, (int)tm.t(), (int)tm.T());
+}
 
 // One V-cycle z = M r.  Levels above kWarpTailCells cells are processed by
 // the whole team; from the first level at or below it the rest of the cycle
@@ -232,17 +292,16 @@ __device__ void team_vcycle(const KArena& A, const KDesc& D, TeamT& tm) {
 // `from_zero`), two passes per step.
 template <int P, class TeamT>
 __device__ void team_cheb0(const KArena& A, const KDesc& D, TeamT& tm, bool from_zero) {
-    const int t = (int)tm.t(), T = (int)tm.T();
     int j = 0;
     if (from_zero) {
-        op_cheb0_first(A, D, t, T, A.cheb_c2[0]);
+        t_cheb0_first(A, D, tm, A.cheb_c2[0]);
         tm.sync();
         j = 1;
     }
     for (; j < A.cheb_k; j++) {
-        op_cheb0_d<P>(A, D, t, T, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
+        t_cheb0_d<P>(A, D, tm, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
         tm.sync();
-        op_cheb0_z(A, D, t, T);
+        t_cheb0_z(A, D, tm);
         tm.sync();
     }
 }
@@ -277,7 +336,7 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
     int l0 = 1;
     while (l0 < L - 1 && D.lev[l0].n > kWarpTailCells) l0++;
     team_cheb0<P>(A, D, tm, true);
-    op_restrict0<P>(A, D, t, T);
+    t_restrict0<P>(A, D, tm);
     tm.sync();
     for (int l = 1; l < l0; l++) {
         team_chebc<P>(A, D, l, tm, true);
@@ -328,7 +387,7 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
     bool conv = false;
     for (outer = 0; outer <= A.max_outer; outer++) {
         double rr = 0.0, bb = 0.0;
-        op_outer_residual(A, D, t, T, rr, bb);
+        t_outer_residual(A, D, tm, rr, bb);
         rr = tm.sum(rr);
         bb = tm.sum(bb);
         bn = sqrt(bb);
@@ -340,30 +399,30 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         const R stop2 = (R)(eta * eta * rr);
         precondition<P>(A, D, tm);
         R rz = 0;
-        op_dot_rz(A, D, t, T, rz);
+        t_dot_rz(A, D, tm, rz);
         rz = tm.sum(rz);
-        op_pupdate(A, D, t, T, 0.0f);
+        t_pupdate(A, D, tm, 0.0f);
         tm.sync();
         for (int it = 0; it < A.max_inner - inner_total; it++) {
             R pq = 0;
-            op_matvec(A, D, t, T, pq);
+            t_matvec(A, D, tm, pq);
             pq = tm.sum(pq);
             const float alpha = pq > (R)0 ? (float)(rz / pq) : 0.0f;
             R rri = 0;
-            op_update(A, D, t, T, alpha, rri);
+            t_update(A, D, tm, alpha, rri);
             rri = tm.sum(rri);
             inner_total++;
             if (rri <= stop2 || !(pq > (R)0)) break;
             precondition<P>(A, D, tm);
             R rzn = 0;
-            op_dot_rz(A, D, t, T, rzn);
+            t_dot_rz(A, D, tm, rzn);
             rzn = tm.sum(rzn);
             const float beta = rz > (R)0 ? (float)(rzn / rz) : 0.0f;
             rz = rzn;
-            op_pupdate(A, D, t, T, beta);
+            t_pupdate(A, D, tm, beta);
             tm.sync();
         }
-        op_accumulate(A, D, t, T);
+        t_accumulate(A, D, tm);
         tm.sync();
     }
     if (tm.leader()) {
@@ -384,8 +443,9 @@ template <int P>
 __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
     k_grid(const __grid_constant__ KArena A, int ngiant) {
     __shared__ SharedScratch sh;
+    __shared__ MarchTile mt;
     GridTeam tm{&sh, reinterpret_cast<unsigned*>(A.queue + 8), reinterpret_cast<unsigned*>(A.queue + 9), A.queue + 10,
-                reinterpret_cast<double*>(A.scratch)};
+                reinterpret_cast<double*>(A.scratch), &mt};
     for (int q = 0; q < ngiant; q++) {
         KDesc& D = A.desc[A.order[q]];
         if (A.fp64_dots) team_solve<P, double>(A, D, tm);

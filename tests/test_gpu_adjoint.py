@@ -174,7 +174,8 @@ def test_whole_gpu_tier_matches_oracle(lib_built):
             e.set_precision(prec)
             # two giant islands (whole-GPU tier, one after the other) and two
             # small ones (persistent kernel) in one solve
-            isls = [synth.noise_island((28, 24, 20), seed=31), synth.solid_block((20, 20, 20), seed=2),
+            # (45 x 37 x 35: several plane-marching work items, odd sides)
+            isls = [synth.noise_island((45, 37, 35), seed=31), synth.solid_block((20, 20, 20), seed=2),
                     synth.noise_island((12, 10, 9), seed=33), synth.noise_island((9, 8, 7), seed=34)]
             isls = [i for i in isls if i.n_active > 0]
             ids, hosts = [], []
