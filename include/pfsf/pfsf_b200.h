@@ -118,6 +118,34 @@ PFSF_API pfsf_result pfsf_adjoint_to_tolerance(pfsf_engine engine, const int32_t
                                                double rel_tol, int32_t max_iter, uint32_t flags,
                                                pfsf_solve_stats* out);
 
+/* Island labelling (no counterpart in the reference C ABI: the reference
+ * labels through its Java/Vulkan label-propagation dispatch,
+ * SH/label_prop_*.comp.glsl, PFSFLabelPropRecorder.java).  One record per
+ * 26-connected component of the non-air voxels -- the reference's 12-uint
+ * component layout (label_prop_summarise_alloc.comp.glsl:57-69). */
+typedef struct pfsf_label_component {
+    uint32_t root_label;  /* 1 + smallest flat index of the component */
+    uint32_t block_count; /* voxels in the component */
+    uint32_t anchored;    /* 1 if any voxel is PFSF_VOXEL_ANCHOR */
+    uint32_t _pad0;
+    uint32_t aabb_min[3]; /* x, y, z */
+    uint32_t _pad1;
+    uint32_t aabb_max[3];
+    uint32_t _pad2;
+} pfsf_label_component;
+
+/* Labels the non-air voxels (uint8 type x lx*ly*lz, host) into 26-connected
+ * components on the GPU.  out_labels (uint32 x N, host, may be NULL): every
+ * voxel's component label = 1 + the smallest flat index in its component
+ * (the fixed point of the reference's hook/jump label propagation),
+ * 0xFFFFFFFF on air.  out_components: the first min(count, capacity)
+ * components in ascending root_label order; *out_count = that number;
+ * *out_overflow = 1 when there were more than capacity components.
+ * Synchronous: returns after the outputs are written. */
+PFSF_API pfsf_result pfsf_label_components(pfsf_engine engine, const uint8_t* voxel_type, int32_t lx, int32_t ly,
+                                           int32_t lz, uint32_t* out_labels, pfsf_label_component* out_components,
+                                           int32_t capacity, int32_t* out_count, int32_t* out_overflow);
+
 /* Diagnostic read of the per-island tick state (not part of the reference
  * ABI; used by parity tests and tooling).  field: 0 phi (float32 x N),
  * 1 history H (float32 x N), 2 damage d (float32 x N), 3 failure flags

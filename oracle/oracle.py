@@ -71,6 +71,8 @@ def lib():
         L.o_kappa_pcg64.restype = i
         L.o_kappa_relres.argtypes = [i, i, i, F64P, U8P, F64P, F32P]
         L.o_kappa_relres.restype = C.c_double
+        L.o_label_components.argtypes = [i, i, i, U8P, U32P, U32P, i]
+        L.o_label_components.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -353,3 +355,50 @@ def flux_loss64(dims, kappa, vtype, phi, rcomp, phi_target):
     gphi[~solid] = 0.0
     gk[t == 0] = 0.0
     return L, gphi.reshape(-1), gk.reshape(-1)
+
+
+# ------------------------------------------------------------- island labels
+NO_ISLAND = 0xFFFFFFFF
+
+
+def label_components(dims, vtype, cap=64):
+    """(labels uint32 [N], components uint32 [min(count, cap), 12], count):
+    breadth-first 26-connected components (oracle/pfsf_oracle.c
+    o_label_components)."""
+    n = int(np.prod(dims))
+    labels = np.zeros(n, np.uint32)
+    comps = np.zeros(max(cap, 1) * 12, np.uint32)
+    cnt = lib().o_label_components(*dims, _c(vtype, np.uint8), labels, comps, int(cap))
+    return labels, comps.reshape(-1, 12)[: min(cnt, cap)], int(cnt)
+
+
+def label_propagation(dims, vtype, max_iters=100000):
+    """The reference's label propagation restated in numpy and run to its
+    fixed point: init label i + 1 on solid/anchor voxels
+    (SH/label_prop_init.comp.glsl:33-50), then alternate a hook pass (each
+    voxel takes the smallest label among itself and its in-box 26 neighbours,
+    label_prop_iterate.comp.glsl:70-93) and a jump pass (label <- label of
+    voxel label - 1 when smaller, :94-104) -- synchronous, as in
+    PFSFLabelPropCpuSimulator.java:115-160 -- until nothing changes.
+    Returns (labels, passes)."""
+    lx, ly, lz = dims
+    t = np.asarray(vtype).reshape(lz, ly, lx)
+    big = np.uint64(1 << 40)
+    lab = np.where(t != 0, np.arange(1, lx * ly * lz + 1, dtype=np.uint64).reshape(lz, ly, lx), big)
+    for it in range(max_iters):
+        pad = np.pad(lab, 1, constant_values=big)
+        m = lab.copy()
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    m = np.minimum(m, pad[1 + dz:1 + dz + lz, 1 + dy:1 + dy + ly, 1 + dx:1 + dx + lx])
+        m = np.where(t != 0, m, big)
+        flat = m.reshape(-1)
+        live = flat != big
+        parent = np.where(live, flat[np.where(live, flat - 1, 0).astype(np.int64)], big)
+        jumped = np.where(live & (parent < flat), parent, flat).reshape(lz, ly, lx)
+        if np.array_equal(jumped, lab):
+            break
+        lab = jumped
+    out = lab.reshape(-1)
+    return np.where(out == big, NO_ISLAND, out).astype(np.uint32), it + 1

@@ -1001,3 +1001,56 @@ double o_kappa_relres(int lx, int ly, int lz, const double *kappa, const uint8_t
     free(x); free(q);
     return bn > 0.0 ? sqrt(rn / bn) : sqrt(rn);
 }
+
+/* ======================= island labelling ======================= */
+/* 26-connected components of the non-air voxels by breadth-first search in
+ * flat order: every voxel gets 1 + the smallest flat index of its component
+ * (the fixed point of SH/label_prop_iterate.comp.glsl's hook/jump
+ * propagation started from label i + 1), 0xFFFFFFFF on air.  comps: up to
+ * cap records of 12 uint32 (label_prop_summarise_alloc.comp.glsl:57-69
+ * layout: root label, block count, anchored, pad, aabb min xyz, pad, aabb
+ * max xyz, pad) in ascending root order.  Returns the number of components. */
+int64_t o_label_components(int lx, int ly, int lz, const uint8_t *type, uint32_t *labels, uint32_t *comps, int cap) {
+    int64_t n = (int64_t)lx * ly * lz;
+    int64_t *queue = malloc((size_t)(n > 0 ? n : 1) * sizeof(int64_t));
+    for (int64_t i = 0; i < n; i++) labels[i] = 0xFFFFFFFFu;
+    int64_t ncomp = 0;
+    for (int64_t s = 0; s < n; s++) {
+        if (type[s] == 0 || labels[s] != 0xFFFFFFFFu) continue;
+        uint32_t lab = (uint32_t)s + 1u;
+        uint32_t cnt = 0, anch = 0, mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0, 0, 0};
+        int64_t head = 0, tail = 0;
+        queue[tail++] = s;
+        labels[s] = lab;
+        while (head < tail) {
+            int64_t c = queue[head++];
+            int x = (int)(c % lx), y = (int)((c / lx) % ly), z = (int)(c / ((int64_t)lx * ly));
+            uint32_t p[3] = {(uint32_t)x, (uint32_t)y, (uint32_t)z};
+            cnt++;
+            if (type[c] == 2) anch = 1;
+            for (int a = 0; a < 3; a++) {
+                if (p[a] < mn[a]) mn[a] = p[a];
+                if (p[a] > mx[a]) mx[a] = p[a];
+            }
+            for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        if (!dx && !dy && !dz) continue;
+                        if (!inb(x + dx, y + dy, z + dz, lx, ly, lz)) continue;
+                        int64_t j = gidx(x + dx, y + dy, z + dz, lx, ly);
+                        if (type[j] == 0 || labels[j] != 0xFFFFFFFFu) continue;
+                        labels[j] = lab;
+                        queue[tail++] = j;
+                    }
+        }
+        if (ncomp < cap) {
+            uint32_t *r = comps + 12 * ncomp;
+            r[0] = lab; r[1] = cnt; r[2] = anch; r[3] = 0;
+            r[4] = mn[0]; r[5] = mn[1]; r[6] = mn[2]; r[7] = 0;
+            r[8] = mx[0]; r[9] = mx[1]; r[10] = mx[2]; r[11] = 0;
+        }
+        ncomp++;
+    }
+    free(queue);
+    return ncomp;
+}

@@ -157,6 +157,7 @@ public:
     pfsf_result debug_read_field(int32_t id, int32_t field, void* out, int64_t bytes, int64_t* out_bytes);
 
     cudaStream_t stream() const { return stream_; }
+    int num_sms() const { return num_sms_; }
     int64_t launches() const { return launches_.load(); }
     void count_launches(int64_t k) { launches_ += k; }
 

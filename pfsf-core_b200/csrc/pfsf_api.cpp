@@ -5,6 +5,7 @@
 #include <new>
 
 #include "engine.h"
+#include "labels.h"
 
 using pfsf_b200::Engine;
 
@@ -182,6 +183,16 @@ PFSF_API pfsf_result pfsf_adjoint_to_tolerance(pfsf_engine e, const int32_t* ids
                                                int32_t max_iter, uint32_t flags, pfsf_solve_stats* out) {
     Engine* g = E(e);
     return g ? g->adjoint_to_tolerance(ids, count, rel_tol, max_iter, flags, out) : PFSF_ERROR_INVALID_ARG;
+}
+
+PFSF_API pfsf_result pfsf_label_components(pfsf_engine e, const uint8_t* type, int32_t lx, int32_t ly, int32_t lz,
+                                           uint32_t* labels, pfsf_label_component* comps, int32_t capacity,
+                                           int32_t* count, int32_t* overflow) {
+    Engine* g = E(e);
+    if (!g) return PFSF_ERROR_INVALID_ARG;
+    if (!g->available()) return PFSF_ERROR_NOT_INIT;
+    return pfsf_b200::labels::label_components(g->stream(), g->num_sms(), type, lx, ly, lz, labels, comps, capacity,
+                                               count, overflow);
 }
 
 PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine e, int32_t id, int32_t field, void* out, int64_t bytes,

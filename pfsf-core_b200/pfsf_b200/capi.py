@@ -131,6 +131,8 @@ def load():
         "pfsf_solve_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
                                      C.POINTER(SolveStats)], C.c_int),
         "pfsf_read_solution64": ([E, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_label_components": ([E, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
         "pfsf_register_island_adjoint": ([E, C.c_int32, C.POINTER(AdjointBuffers)], C.c_int),
         "pfsf_adjoint_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
                                        C.POINTER(SolveStats)], C.c_int),
@@ -219,6 +221,17 @@ class Engine:
         rc = self.L.pfsf_solve_to_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, tol,
                                             max_iter, flags, C.byref(st))
         return rc, st
+
+    def label_components(self, vtype, dims, capacity=64, labels=True):
+        """26-connected components of the non-air voxels on the GPU:
+        (rc, labels uint32 [N] or None, components uint32 [count, 12], count, overflow)."""
+        vt = np.ascontiguousarray(vtype, np.uint8)
+        lab = np.zeros(int(np.prod(dims)), np.uint32) if labels else None
+        comps = np.zeros((max(capacity, 1), 12), np.uint32)
+        cnt, ovf = C.c_int32(0), C.c_int32(0)
+        rc = self.L.pfsf_label_components(self.h, _ptr(vt), *dims, None if lab is None else _ptr(lab), _ptr(comps),
+                                          capacity, C.byref(cnt), C.byref(ovf))
+        return rc, lab, comps[: cnt.value], cnt.value, ovf.value
 
     def register_adjoint(self, iid, grad_phi, grad_source, grad_kappa):
         arrs = [grad_phi, grad_source, grad_kappa]
