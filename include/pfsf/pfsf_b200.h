@@ -80,6 +80,25 @@ PFSF_API pfsf_result pfsf_solve_to_tolerance(pfsf_engine engine, const int32_t* 
                                              double rel_tol, int32_t max_iter, uint32_t flags,
                                              pfsf_solve_stats* out);
 
+/* pfsf_tick_dbb with the fixed 16-step schedule (pfsf_engine.cpp:484)
+ * replaced by the tolerance solve: every listed island must have both the
+ * reference buffers (pfsf_register_island_buffers: face conductivity,
+ * rcomp, rtens, max_phi, type ...) and the kappa-form buffers
+ * (pfsf_register_island_kappa); all of them are solved to rel_tol in one
+ * batched solve (phi written back to the kappa phi array, which is also the
+ * next tick's starting guess), then on that phi: the history update
+ * H = max(H, psi_e) (rbgs_smooth.comp.glsl:177-191), the phase field, the
+ * failure scan and the failure compaction of the reference tick, with the
+ * {count}{x,y,z,type} tuples appended to failure_addr exactly as
+ * pfsf_tick_dbb does (count pre-zeroed) and phi copied to the stress
+ * readback buffer when one is registered.  Listed islands are processed
+ * whether or not they are marked dirty; the reference-layout buffers are
+ * re-uploaded for dirty islands (as pfsf_tick_dbb does), the kappa-form
+ * buffers on every call.  out may be NULL. */
+PFSF_API pfsf_result pfsf_tick_tolerance(pfsf_engine engine, const int32_t* island_ids, int32_t count,
+                                         int64_t epoch, void* failure_addr, int64_t failure_bytes, double rel_tol,
+                                         int32_t max_iter, pfsf_solve_stats* out);
+
 /* Copies the FP64 solution accumulator of the last tolerance solve of an
  * island (count = min(N, capacity) values).  The FP32 phi written back by
  * pfsf_solve_to_tolerance is this vector rounded to float32. */

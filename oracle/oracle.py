@@ -71,6 +71,7 @@ def lib():
         L.o_kappa_pcg64.restype = i
         L.o_kappa_relres.argtypes = [i, i, i, F64P, U8P, F64P, F32P]
         L.o_kappa_relres.restype = C.c_double
+        L.o_history.argtypes = [i, i, i, F32P, F32P, U8P, F32P]
         L.o_label_components.argtypes = [i, i, i, U8P, U32P, U32P, i]
         L.o_label_components.restype = C.c_int64
         _lib = L
@@ -160,6 +161,26 @@ def failure_scan(dims, phi, sigma, maxphi, rcomp, vtype, fail, rtens, macro, rho
     lib().o_failure_scan(*dims, _c(phi, np.float32), _c(sigma, np.float32), _c(maxphi, np.float32),
                          _c(rcomp, np.float32), _c(vtype, np.uint8), fail, _c(rtens, np.float32), macro,
                          _c(rho, np.float32), phi_orphan)
+
+
+def history(dims, phi, sigma, vtype, H):
+    lib().o_history(*dims, _c(phi, np.float32), _c(sigma, np.float32), _c(vtype, np.uint8), H)
+
+
+def tolerance_tick_tail(dims, phi32, case, H, D, fail):
+    """The tail of the tolerance tick on a given FP32 phi: history update,
+    phase field (D snapshot), failure scan -- in place on H, D, fail.
+    `case` holds the reference-layout inputs (conductivity, type, rcomp,
+    rtens, max_phi, hydration, source).  Returns the macro residual array."""
+    n = int(np.prod(dims))
+    history(dims, phi32, case["conductivity"], case["type"], H)
+    phase_field(dims, phi32, H, D, case["conductivity"], case["type"], fail, case["hydration"])
+    mb = [(v + 7) // 8 for v in dims]
+    macro = np.full(mb[0] * mb[1] * mb[2], 0x38D1B717, np.uint32)
+    failure_scan(dims, phi32, case["conductivity"], case["max_phi"], case["rcomp"], case["type"], fail,
+                 case["rtens"], macro, case["source"])
+    assert fail.size == n
+    return macro
 
 
 # ---------------------------------------------------------------- island state

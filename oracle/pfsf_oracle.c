@@ -160,6 +160,26 @@ static float amor_psi(const float *sigma, int64_t N, int64_t i, const float nphi
     return 0.5f * phi_new * phi_new * k_comp;
 }
 
+/* ---- history update H = max(H, psi_e(phi)) on solid voxels with phi > 0,
+ * the update rbgs_smooth.comp.glsl:177-191 performs inside each sweep, applied
+ * once to a given phi (the tolerance tick) ---- */
+void o_history(int lx, int ly, int lz, const float *phi, const float *sigma, const uint8_t *type, float *H) {
+    int64_t N = (int64_t)lx * ly * lz;
+    static const int F6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                int64_t i = gidx(x, y, z, lx, ly);
+                if (type[i] != 1 || !(phi[i] > 0.0f)) continue;
+                float nphi6[6];
+                for (int d = 0; d < 6; d++) {
+                    int nx = x + F6[d][0], ny = y + F6[d][1], nz = z + F6[d][2];
+                    nphi6[d] = inb(nx, ny, nz, lx, ly, lz) ? phi[gidx(nx, ny, nz, lx, ly)] : 0.0f;
+                }
+                H[i] = fmaxf(H[i], amor_psi(sigma, N, i, nphi6, x, y, z, lx, ly, lz, phi[i]));
+            }
+}
+
 /* ---- rbgs_smooth.comp.glsl:73-211, one colour pass, in place ---- */
 void o_rbgs_color(int lx, int ly, int lz, float *phi, const float *rho, const float *sigma,
                   const uint8_t *type, float *H, const uint32_t *macro, int color, float damping) {

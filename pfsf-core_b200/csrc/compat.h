@@ -31,6 +31,8 @@ void finalize(cudaStream_t s, const float* partial, int64_t count, float* red, i
 void phase_field(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* H, float* D,
                  const float* Dold, const float* sigma, const uint8_t* type, uint8_t* fail, const float* hyd,
                  float l0, float gc, float relax, int split);
+void history(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const uint8_t* type,
+             float* H);
 void failure_scan(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const float* rcomp,
                   const uint8_t* type, uint8_t* fail, const float* rtens, uint32_t* macro, const float* rho);
 void macro_fill(cudaStream_t s, uint32_t* macro, int64_t nmb);

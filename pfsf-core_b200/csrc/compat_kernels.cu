@@ -137,6 +137,30 @@ __global__ void __launch_bounds__(kBlock) k_rbgs_color(int lx, int ly, int lz, f
     phi[i] = result;
 }
 
+// ---------------------------------------------------------------- history
+// H = max(H, psi_e(phi)) on solid voxels with phi > 0 -- the history update
+// the reference performs inside every RBGS / Jacobi sweep
+// (SH/rbgs_smooth.comp.glsl:177-191), applied once to a given phi (the
+// tolerance tick, whose phi does not come from sweeps).
+__global__ void __launch_bounds__(kBlock) k_history(int lx, int ly, int lz, const float* __restrict__ phi,
+                                                    const float* __restrict__ sigma,
+                                                    const uint8_t* __restrict__ type, float* __restrict__ H) {
+    const int64_t n = (int64_t)lx * ly * lz;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || type[i] != kSolid) return;
+    const float p = phi[i];
+    if (!(p > 0.0f)) return;
+    const int x = (int)(i % lx), y = (int)((i / lx) % ly), z = (int)(i / ((int64_t)lx * ly));
+    float s6[6], nphi6[6];
+    load_s6(sigma, n, i, s6);
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+        const int nx = x + kOfs(d, 0), ny = y + kOfs(d, 1), nz = z + kOfs(d, 2);
+        nphi6[d] = inb(nx, ny, nz, lx, ly, lz) ? phi[gidx(nx, ny, nz, lx, ly)] : 0.0f;
+    }
+    H[i] = fmaxf(H[i], amor_psi(s6, nphi6, x, y, z, lx, ly, lz, p));
+}
+
 // ---------------------------------------------------------------- coarse Jacobi
 // SH/jacobi_smooth.comp.glsl:60-227, omega = 1, reading phi_in (a snapshot)
 // and writing every voxel of phi_out.  Hfine is the fine-level history buffer,
@@ -870,6 +894,10 @@ void phase_field(cudaStream_t s, int lx, int ly, int lz, const float* phi, const
                  float l0, float gc, float relax, int split) {
     k_phase_field<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, H, D, Dold, sigma, type, fail,
                                                                      hyd, l0, gc, relax, split);
+}
+void history(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const uint8_t* type,
+             float* H) {
+    k_history<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, sigma, type, H);
 }
 void failure_scan(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const float* rcomp,
                   const uint8_t* type, uint8_t* fail, const float* rtens, uint32_t* macro, const float* rho) {

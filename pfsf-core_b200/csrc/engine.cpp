@@ -516,33 +516,59 @@ pfsf_result Engine::tick(const int32_t* ids, int32_t count, pfsf_tick_result* re
         compat::macro_fill(stream_, s->macro, s->nmb);
         launches_++;
         solve_steps(*s, kStepsMajor);
-        if (cfg_.enable_phase_field) {
-            cudaMemcpyAsync(s->Dold, s->D, (size_t)s->n * 4, cudaMemcpyDeviceToDevice, stream_);
-            compat::phase_field(stream_, s->lx, s->ly, s->lz, s->phi, s->H, s->D, s->Dold, s->sigma, s->type, s->fail,
-                                s->hyd, kPfL0, kPfGc, kPfRelax, 1);
-            launches_++;
-        }
-        compat::failure_scan(stream_, s->lx, s->ly, s->lz, s->phi, s->sigma, s->rcomp, s->type, s->fail, s->rtens,
-                             s->macro, s->src);
-        compat::macro_max(stream_, s->macro, s->nmb, &s->result->macro_max);
-        launches_ += 2;
-        if (want_cap > 0) {
-            if (s->tuple_cap < want_cap) {
-                s->tuples = (int32_t*)dalloc(*s, (size_t)want_cap * 16);
-                if (!s->tuples) return PFSF_ERROR_OUT_OF_VRAM;
-                s->tuple_cap = want_cap;
-            }
-            compat::fail_compact(stream_, s->fail, s->lx, s->ly, s->lz, s->origin.x, s->origin.y, s->origin.z,
-                                 s->fcounts, s->foffsets, &s->result->fail_total, s->tuples, want_cap);
-            launches_ += 3;
-        }
-        if (s->hosts.stress_out && s->hosts.stress_bytes > 0) {
-            const int64_t nf = std::min<int64_t>(s->n, s->hosts.stress_bytes / 4);
-            if (!CU_OK(cudaMemcpyAsync(s->hosts.stress_out, s->phi, (size_t)nf * 4, cudaMemcpyDeviceToHost, stream_)))
-                return PFSF_ERROR_VULKAN;
-        }
+        if (pfsf_result rc = enqueue_tail(*s, want_cap); rc != PFSF_OK) return rc;
         dispatched.push_back(s);
     }
+    if (pfsf_result rc = finish_dispatch(dispatched, drain, fail_addr, dbb_count, dbb_cap, result, legacy_cap);
+        rc != PFSF_OK)
+        return rc;
+    const auto t1 = std::chrono::steady_clock::now();
+    {
+        std::lock_guard<std::mutex> lk(stats_mtx_);
+        last_tick_ms_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    }
+    return PFSF_OK;
+}
+
+// The reference tick's tail on the island's current phi: phase field (with
+// its D snapshot), failure scan, macro-residual max, failure compaction into
+// device tuples, stress readback (pfsf_engine.cpp:513-560).
+pfsf_result Engine::enqueue_tail(Island& is, int32_t want_cap) {
+    Island* s = &is;
+    if (cfg_.enable_phase_field) {
+        cudaMemcpyAsync(s->Dold, s->D, (size_t)s->n * 4, cudaMemcpyDeviceToDevice, stream_);
+        compat::phase_field(stream_, s->lx, s->ly, s->lz, s->phi, s->H, s->D, s->Dold, s->sigma, s->type, s->fail,
+                            s->hyd, kPfL0, kPfGc, kPfRelax, 1);
+        launches_++;
+    }
+    compat::failure_scan(stream_, s->lx, s->ly, s->lz, s->phi, s->sigma, s->rcomp, s->type, s->fail, s->rtens,
+                         s->macro, s->src);
+    compat::macro_max(stream_, s->macro, s->nmb, &s->result->macro_max);
+    launches_ += 2;
+    if (want_cap > 0) {
+        if (s->tuple_cap < want_cap) {
+            s->tuples = (int32_t*)dalloc(*s, (size_t)want_cap * 16);
+            if (!s->tuples) return PFSF_ERROR_OUT_OF_VRAM;
+            s->tuple_cap = want_cap;
+        }
+        compat::fail_compact(stream_, s->fail, s->lx, s->ly, s->lz, s->origin.x, s->origin.y, s->origin.z,
+                             s->fcounts, s->foffsets, &s->result->fail_total, s->tuples, want_cap);
+        launches_ += 3;
+    }
+    if (s->hosts.stress_out && s->hosts.stress_bytes > 0) {
+        const int64_t nf = std::min<int64_t>(s->n, s->hosts.stress_bytes / 4);
+        if (!CU_OK(cudaMemcpyAsync(s->hosts.stress_out, s->phi, (size_t)nf * 4, cudaMemcpyDeviceToHost, stream_)))
+            return PFSF_ERROR_VULKAN;
+    }
+    return PFSF_OK;
+}
+
+// Reads the dispatched islands' tick results back and appends their failure
+// tuples to the caller's buffers in island order, voxel order
+// (island_buffer.cpp:864-966).
+pfsf_result Engine::finish_dispatch(const std::vector<Island*>& dispatched, bool drain, void* fail_addr,
+                                    int32_t dbb_count, int32_t dbb_cap, pfsf_tick_result* result,
+                                    int32_t legacy_cap) {
     if (!dispatched.empty()) {
         if ((int)dispatched.size() > host_results_cap_) {
             cudaFreeHost(host_results_);
@@ -581,11 +607,6 @@ pfsf_result Engine::tick(const int32_t* ids, int32_t count, pfsf_tick_result* re
         if (any_copy && !CU_OK(cudaStreamSynchronize(stream_))) return PFSF_ERROR_VULKAN;
         if (drain) *static_cast<int32_t*>(fail_addr) = dbb_count;
         if (result) result->count = legacy_count;
-    }
-    const auto t1 = std::chrono::steady_clock::now();
-    {
-        std::lock_guard<std::mutex> lk(stats_mtx_);
-        last_tick_ms_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
     }
     return PFSF_OK;
 }

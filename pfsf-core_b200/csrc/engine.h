@@ -151,6 +151,8 @@ public:
     pfsf_result solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter, uint32_t flags,
                                    pfsf_solve_stats* out);
     pfsf_result read_solution64(int32_t id, double* out, int64_t cap, int64_t* count);
+    pfsf_result tick_tolerance(const int32_t* ids, int32_t count, void* fail_addr, int64_t fail_bytes, double tol,
+                               int32_t max_iter, pfsf_solve_stats* out);
     pfsf_result register_adjoint(int32_t id, const pfsf_island_adjoint_buffers* b);
     pfsf_result adjoint_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
                                      uint32_t flags, pfsf_solve_stats* out);
@@ -176,6 +178,9 @@ private:
     pfsf_result run_solve(const KArena& k, std::vector<KDesc>& res, int64_t& launches);
     bool grid_barrier_failed() const;
     void fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_solve_stats& st) const;
+    pfsf_result enqueue_tail(Island& isl, int32_t want_cap);
+    pfsf_result finish_dispatch(const std::vector<Island*>& dispatched, bool drain, void* fail_addr, int32_t dbb_count,
+                                int32_t dbb_cap, pfsf_tick_result* result, int32_t legacy_cap);
     bool upload(Island& isl);
     bool ensure_mg(Island& isl);
     bool ensure_pcg(Island& isl);

@@ -5,6 +5,7 @@
 #include <numeric>
 
 #include "arena.h"
+#include "compat.h"
 
 namespace pfsf_b200 {
 
@@ -493,6 +494,52 @@ pfsf_result Engine::read_solution64(int32_t id, double* out, int64_t cap, int64_
         !CU_OK(cudaStreamSynchronize(stream_)))
         return PFSF_ERROR_VULKAN;
     *count = n;
+    return PFSF_OK;
+}
+
+// The reference tick with its fixed 16-step schedule replaced by the
+// tolerance solve: solve every listed island to rel. tolerance (one batched
+// launch), put the FP32 phi into the island's reference-layout buffers, apply
+// the history update H = max(H, psi_e(phi)) the reference performs inside its
+// sweeps, then the reference tick's tail (phase field, failure scan, failure
+// compaction, stress readback) and append failures to the caller's buffer.
+pfsf_result Engine::tick_tolerance(const int32_t* ids, int32_t count, void* fail_addr, int64_t fail_bytes, double tol,
+                                   int32_t max_iter, pfsf_solve_stats* out) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (count < 0 || (count > 0 && !ids) || !(tol > 0.0)) return PFSF_ERROR_INVALID_ARG;
+    const bool drain = fail_addr != nullptr && fail_bytes >= 20;
+    if (fail_addr && fail_bytes >= 4) *static_cast<int32_t*>(fail_addr) = 0;
+    const int32_t dbb_cap = drain ? (int32_t)((fail_bytes - 4) / 16) : 0;
+    std::vector<Island*> set;
+    if (!collect_kappa_set(ids, count, set)) return PFSF_ERROR_INVALID_ARG;
+    std::vector<int32_t> sids;
+    for (Island* s : set) {
+        if (!s->hosts.registered) return PFSF_ERROR_INVALID_ARG;
+        if (!ensure_compat(*s)) return PFSF_ERROR_OUT_OF_VRAM;
+        if (s->dirty && !upload(*s)) return PFSF_ERROR_VULKAN;  // as pfsf_tick_dbb: dirty islands re-upload
+        sids.push_back(s->id);
+    }
+    pfsf_solve_stats st{};
+    st.struct_bytes = (int32_t)sizeof(st);
+    if (set.empty()) {
+        if (out) *out = st;
+        return PFSF_OK;
+    }
+    if (pfsf_result rc = solve_to_tolerance(sids.data(), (int32_t)sids.size(), tol, max_iter, 0, &st); rc != PFSF_OK)
+        return rc;
+    const Arena& A = *arena_;
+    for (size_t q = 0; q < set.size(); q++) {
+        Island* s = set[q];
+        if (!CU_OK(cudaMemcpyAsync(s->phi, A.dev.e + A.desc[q].off, (size_t)s->n * 4, cudaMemcpyDeviceToDevice,
+                                   stream_)))
+            return PFSF_ERROR_VULKAN;
+        compat::macro_fill(stream_, s->macro, s->nmb);
+        compat::history(stream_, s->lx, s->ly, s->lz, s->phi, s->sigma, s->type, s->H);
+        launches_ += 2;
+        if (pfsf_result rc = enqueue_tail(*s, dbb_cap); rc != PFSF_OK) return rc;
+    }
+    if (pfsf_result rc = finish_dispatch(set, drain, fail_addr, 0, dbb_cap, nullptr, 0); rc != PFSF_OK) return rc;
+    if (out) *out = st;
     return PFSF_OK;
 }
 

@@ -169,6 +169,13 @@ PFSF_API pfsf_result pfsf_solve_to_tolerance(pfsf_engine e, const int32_t* ids, 
     return g ? g->solve_to_tolerance(ids, count, rel_tol, max_iter, flags, out) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_tick_tolerance(pfsf_engine e, const int32_t* ids, int32_t count, int64_t, void* fail_addr,
+                                         int64_t fail_bytes, double rel_tol, int32_t max_iter, pfsf_solve_stats* out) {
+    if (fail_addr && fail_bytes >= (int64_t)sizeof(int32_t)) *static_cast<int32_t*>(fail_addr) = 0;
+    Engine* g = E(e);
+    return g ? g->tick_tolerance(ids, count, fail_addr, fail_bytes, rel_tol, max_iter, out) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine e, int32_t id, double* out, int64_t cap, int64_t* count) {
     Engine* g = E(e);
     return g ? g->read_solution64(id, out, cap, count) : PFSF_ERROR_INVALID_ARG;

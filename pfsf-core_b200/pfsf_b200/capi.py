@@ -131,6 +131,8 @@ def load():
         "pfsf_solve_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
                                      C.POINTER(SolveStats)], C.c_int),
         "pfsf_read_solution64": ([E, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_tick_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
+                                 C.c_int32, C.POINTER(SolveStats)], C.c_int),
         "pfsf_label_components": ([E, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
         "pfsf_register_island_adjoint": ([E, C.c_int32, C.POINTER(AdjointBuffers)], C.c_int),
@@ -220,6 +222,16 @@ class Engine:
         st = SolveStats()
         rc = self.L.pfsf_solve_to_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, tol,
                                             max_iter, flags, C.byref(st))
+        return rc, st
+
+    def tick_tolerance(self, ids, failure_buf=None, tol=1e-6, max_iter=500, epoch=0):
+        """pfsf_tick_tolerance: tolerance solve + the reference tick's tail."""
+        ids = np.ascontiguousarray(ids, np.int32)
+        st = SolveStats()
+        rc = self.L.pfsf_tick_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, epoch,
+                                        None if failure_buf is None else _ptr(failure_buf),
+                                        0 if failure_buf is None else failure_buf.nbytes, tol, max_iter,
+                                        C.byref(st))
         return rc, st
 
     def label_components(self, vtype, dims, capacity=64, labels=True):
