@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch", "single", "adjoint"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "single", "adjoint", "fracture"], default="batch")
+    ap.add_argument("--ticks", type=int, default=200, help="fracture workload: ticks")
     ap.add_argument("--fd-voxels", type=int, default=256)
     ap.add_argument("--dims", default="256,256,128", help="single workload: island sides x,y,z")
     ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
@@ -380,7 +381,8 @@ def run_ours(args):
             "speedup_vs_plain_fp32": (plain_ms / ms) if plain_ms else None,
             "inner_iterations_total": int(stats[-1].inner_iterations_total),
             "schedule": {"island_ms_sum": stats[-1].island_ms_sum, "island_ms_max": stats[-1].island_ms_max,
-                         "span_ms": stats[-1].span_ms,
+                         "span_ms": stats[-1].span_ms, "setup_ms_sum": stats[-1].setup_ms_sum,
+                         "precond_ms_sum": stats[-1].precond_ms_sum,
                          "cluster": os.environ.get("PFSF_CLUSTER", "16"),
                          "cluster_min_voxels": os.environ.get("PFSF_CLUSTER_MIN_VOXELS", "131072"),
                          "warp_max_voxels": os.environ.get("PFSF_WARP_MAX_VOXELS", "0"),
@@ -468,12 +470,105 @@ def run_adjoint(args):
     eng.close()
 
 
+def run_fracture(args):
+    """Fracture run: one noise island (default 512x512x256, 55 % occupancy),
+    --ticks tolerance ticks (pfsf_tick_tolerance: solve to 1e-6, history
+    H = max(H, psi_e), phase field, failure scan, failure compaction) with the
+    load ramped linearly 1x -> 2x, face conductivity = the kappa link value.
+    Runs the mixed-precision batched solve and then the plain FP32 per-island
+    solve on fresh state and compares final damage and failure codes."""
+    os.environ.setdefault("PFSF_GRID_MIN_VOXELS", str(1 << 21))
+    from pfsf_b200 import capi, synth
+
+    dims = tuple(int(v) for v in args.dims.split(","))
+    t0 = time.perf_counter()
+    isl = synth.noise_island(dims, seed=51, occupancy=0.55)
+    sig = synth.face_sigma_from_kappa(isl.dims, isl.vtype, isl.kappa)
+    t_gen = time.perf_counter() - t0
+    eng = capi.Engine(capi.default_config(max_island_size=1 << 30, tick_budget_ms=1 << 30, vram=180 << 30))
+    if eng.init() != capi.PFSF_OK:
+        raise RuntimeError("pfsf_init failed")
+    n = isl.n
+    rcomp = isl.rcomp.astype(np.float32)
+    rtens = isl.rtens.astype(np.float32)
+    maxphi = np.full(n, 1e9, np.float32)
+    cap = 1 << 20
+    runs = {}
+    scale = None
+    for name, mode, prec in (("mixed", capi.SOLVE_BATCHED, {"bf16": capi.PREC_BF16, "fp16": capi.PREC_FP16,
+                                                              "fp32": capi.PREC_FP32}[args.precision]),
+                             ("plain_fp32", capi.SOLVE_PER_ISLAND, capi.PREC_FP32)):
+        if name == "plain_fp32" and args.no_plain:
+            continue
+        iid = len(runs) + 1
+        assert eng.add_island(iid, isl.dims) == capi.PFSF_OK
+        phi = np.zeros(n, np.float32)
+        phik = np.zeros(n, np.float32)
+        src = isl.source.copy()
+        assert eng.register_buffers(iid, phi, src, sig, isl.vtype, rcomp, rtens, maxphi) == capi.PFSF_OK
+        assert eng.register_kappa(iid, phik, src, isl.kappa, isl.vtype) == capi.PFSF_OK
+        eng.set_solve_mode(mode)
+        eng.set_precision(prec)
+        if scale is None:  # loads scaled so max phi = 20 at 1x: the phase field and the scan act
+            rc, st = eng.solve([iid], tol=1e-6, flags=capi.SOLVE_COLD_START)
+            scale = 20.0 / float(np.abs(phik).max())
+            phik[:] = 0.0
+        base = (isl.source * np.float32(scale)).astype(np.float32)
+        fb = np.zeros(1 + 4 * cap, np.int32)
+        wall, dev, fails, iters, rel = [], [], [], [], 0.0
+        for t in range(args.ticks):
+            src[:] = base * np.float32(1.0 + t / max(args.ticks - 1, 1))
+            eng.L.pfsf_mark_full_rebuild(eng.h, iid)  # the Java runtime marks islands dirty every tick
+            t1 = time.perf_counter()
+            rc, st = eng.tick_tolerance([iid], fb, tol=args.tol)
+            wall.append((time.perf_counter() - t1) * 1000.0)
+            if rc != capi.PFSF_OK or st.islands_converged != 1:
+                raise RuntimeError(f"tick {t}: rc={rc} relres={st.max_rel_residual}")
+            dev.append(st.device_ms)
+            fails.append(int(fb[0]))
+            iters.append(int(st.inner_iterations_total))
+            rel = max(rel, st.max_rel_residual)
+        runs[name] = {"D": eng.debug_field(iid, 2), "fail": eng.debug_field(iid, 3), "wall": wall, "dev": dev,
+                      "fails": fails, "iters": iters, "relres": rel}
+        eng.L.pfsf_remove_island(eng.h, iid)
+    m = runs["mixed"]
+    line = {
+        "metric": "config-5 fracture: ms per tolerance tick (solve to 1e-6 + history + phase field + failure scan)",
+        "value": float(np.mean(m["wall"])), "unit": "ms/tick", "higher_is_better": False, "n_gpus": 1,
+        "data": "synthetic", "dtype": "f32",
+        "config": {"workload": f"one {args.dims.replace(',', 'x')} noise island (55 % occupancy, anchored "
+                               f"component), {args.ticks} ticks, load ramped 1x->2x, warm start",
+                   "grid_voxels": n, "active_voxels": int(isl.n_active), "precision": args.precision,
+                   "tol": args.tol, "generation_s": t_gen},
+        "solve_device_ms_mean": float(np.mean(m["dev"])), "inner_iterations_mean": float(np.mean(m["iters"])),
+        "max_rel_residual_fp64": m["relres"], "failures_last_tick": m["fails"][-1],
+        "failures_first_tick": m["fails"][0], "damage_max": float(m["D"].max()),
+    }
+    if "plain_fp32" in runs:
+        p = runs["plain_fp32"]
+        line["plain_fp32_ms_per_tick"] = float(np.mean(p["wall"]))
+        line["plain_fp32_solve_device_ms_mean"] = float(np.mean(p["dev"]))
+        line["speedup_vs_plain_fp32"] = line["plain_fp32_ms_per_tick"] / line["value"]
+        line["failure_code_agreement"] = float(np.mean(m["fail"] == p["fail"]))
+        line["failure_code_mismatches"] = int(np.sum(m["fail"] != p["fail"]))
+        dd = np.abs(m["D"] - p["D"])
+        line["damage_max_abs_diff"] = float(dd.max())
+        # psi_e switches by 100x where flux_in crosses 3 flux_out (rbgs_smooth.comp.glsl:186):
+        # voxels on that switch can differ between two solves that agree to 1e-6
+        line["damage_voxels_differing_1e-3"] = int(np.sum(dd > 1e-3))
+        line["damage_voxels"] = int(np.sum((m["D"] > 0) | (p["D"] > 0)))
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "fracture":
+        run_fracture(args)
     else:
         run_ours(args)
 

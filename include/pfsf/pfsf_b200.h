@@ -64,6 +64,8 @@ typedef struct pfsf_solve_stats {
     double island_ms_sum;           /* batched mode: sum over islands of solve time */
     double island_ms_max;           /* batched mode: longest single island solve */
     double span_ms;                 /* batched mode: first island start to last island end */
+    double setup_ms_sum;            /* batched mode: sum over islands of the hierarchy build */
+    double precond_ms_sum;          /* batched mode: sum over islands of the time in V-cycles */
 } pfsf_solve_stats;
 
 /* Registers the kappa-form inputs of an island created by pfsf_add_island.

@@ -5,6 +5,11 @@
 
 namespace pfsf_b200 {
 
+// Levels of the hierarchy (fine + 4 coarse).  Measured with 8 (coarsest
+// levels of <= 64 cells): the 256x256x128 island took as many PCG iterations
+// and 6 % longer per tick (the extra levels run on one warp while the rest of
+// the GPU waits), so the coarsest level of a giant island stays large and is
+// smoothed by the whole team.
 constexpr int kMaxLevels = 5;
 
 struct KLevel {
@@ -25,6 +30,7 @@ struct KDesc {
     double bnorm;
     int inner_iters, outer_iters, converged, status;
     unsigned long long t_start, t_end;  // %globaltimer (ns) around the island's solve
+    unsigned long long t_setup, t_precond;  // ns in the hierarchy build / in V-cycles (batched mode)
 };
 
 // Device pointers and parameters of one batched solve.
@@ -39,6 +45,7 @@ struct KArena {
     uint16_t* coef16;      // coarse off-diagonals, 26 per cell (16-bit)
     float* coef32;         // coarse off-diagonals, 26 per cell (FP32)
     float *cx, *cb;        // coarse solution / right-hand side
+    float* cx2;            // second coarse solution array (out-of-place Chebyshev steps)
     KDesc* desc;
     const int* order;      // island processing order (largest first)
     int* queue;            // work counter

@@ -226,19 +226,20 @@ __device__ __forceinline__ void t_restrict0(const KArena& A, const KDesc& D, Tea
     else op_restrict0<P>(A, D, (int)tm.t(), (int)tm.T());
 }
 template <class TeamT>
-__device__ __forceinline__ void t_cheb0_first(const KArena& A, const KDesc& D, TeamT& tm, float c2) {
-    if constexpr (TeamT::kMarch) vop_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2);
-    else op_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2);
+__device__ __forceinline__ void t_cheb0_first(const KArena& A, const KDesc& D, TeamT& tm, float c2, float* zout) {
+    if constexpr (TeamT::kMarch) vop_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2, zout);
+    else op_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2, zout);
 }
 template <int P, class TeamT>
-__device__ __forceinline__ void t_cheb0_d(const KArena& A, const KDesc& D, TeamT& tm, float c1, float c2) {
-    if constexpr (TeamT::kMarch) mop_cheb0_d<P>(A, D, *tm.mt, tm.cta(), tm.ncta(), c1, c2);
-    else op_cheb0_d<P>(A, D, (int)tm.t(), (int)tm.T(), c1, c2);
+__device__ __forceinline__ void t_cheb0_dz(const KArena& A, const KDesc& D, TeamT& tm, const float* zin, float* zout,
+                                           float c1, float c2) {
+    if constexpr (TeamT::kMarch) mop_cheb0_dz<P>(A, D, *tm.mt, tm.cta(), tm.ncta(), zin, zout, c1, c2);
+    else op_cheb0_dz<P>(A, D, (int)tm.t(), (int)tm.T(), zin, zout, c1, c2);
 }
 template <class TeamT>
-__device__ __forceinline__ void t_cheb0_z(const KArena& A, const KDesc& D, TeamT& tm) {
-    if constexpr (TeamT::kMarch) vop_cheb0_z(A, D, (int)tm.t(), (int)tm.T());
-    else op_cheb0_z(A, D, (int)tm.t(), (int)tm.T());
+__device__ __forceinline__ void t_copy(const KDesc& D, TeamT& tm, const float* src, float* dst) {
+    if constexpr (TeamT::kMarch) vop_copy((int)tm.t(), (int)tm.T(), (int)D.n, src, dst);
+    else op_copy((int)tm.t(), (int)tm.T(), (int)D.n, src, dst);
 }
 
 // One V-cycle z = M r.  Levels above kWarpTailCells cells are processed by
@@ -289,41 +290,85 @@ __device__ void team_vcycle(const KArena& A, const KDesc& D, TeamT& tm) {
 }
 
 // Chebyshev smoothing of degree A.cheb_k on the fine level (from z = 0 when
-// `from_zero`), two passes per step.
+// `from_zero`), one pass per step: the steps ping-pong z between the z array
+// and the q array (free while the preconditioner runs).  z is in the z array
+// on exit; on entry it is in the z array, or in q when `in_q`.  From zero, the
+// first step writes whichever array makes the last step land in z.
 template <int P, class TeamT>
-__device__ void team_cheb0(const KArena& A, const KDesc& D, TeamT& tm, bool from_zero) {
+__device__ void team_cheb0(const KArena& A, const KDesc& D, TeamT& tm, bool from_zero, bool in_q = false) {
+    float* zz = A.z + D.off;
+    float* zq = A.q + D.off;
+    bool cur_q = in_q;
     int j = 0;
     if (from_zero) {
-        t_cheb0_first(A, D, tm, A.cheb_c2[0]);
+        cur_q = ((A.cheb_k - 1) & 1) != 0;
+        t_cheb0_first(A, D, tm, A.cheb_c2[0], cur_q ? zq : zz);
         tm.sync();
         j = 1;
     }
     for (; j < A.cheb_k; j++) {
-        t_cheb0_d<P>(A, D, tm, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
+        t_cheb0_dz<P>(A, D, tm, cur_q ? zq : zz, cur_q ? zz : zq, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
         tm.sync();
-        t_cheb0_z(A, D, tm);
+        cur_q = !cur_q;
+    }
+    if (cur_q) {
+        t_copy(D, tm, zq, zz);
         tm.sync();
     }
 }
 template <int P, class TeamT>
-__device__ void team_chebc(const KArena& A, const KDesc& D, int l, TeamT& tm, bool from_zero) {
+__device__ void team_chebc(const KArena& A, const KDesc& D, int l, TeamT& tm, bool from_zero, bool in_x2 = false) {
+    // as team_cheb0, ping-ponging the level's x and x2 arrays; x on exit
     const int t = (int)tm.t(), T = (int)tm.T();
+    float* xa = A.cx + D.lev[l].off;
+    float* xb = A.cx2 + D.lev[l].off;
+    const int n = (int)D.lev[l].n;
+    bool cur_b = in_x2;
     int j = 0;
     if (from_zero) {
-        op_chebc_first(A, D, l, t, T, A.cheb_c2[0]);
+        cur_b = ((A.cheb_k - 1) & 1) != 0;
+        op_chebc_first(A, D, l, t, T, A.cheb_c2[0], cur_b ? xb : xa);
         tm.sync();
         j = 1;
     }
     for (; j < A.cheb_k; j++) {
-        op_chebc_d<P>(A, D, l, t, T, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
+        op_chebc_dx<P>(A, D, l, t, T, cur_b ? xb : xa, cur_b ? xa : xb, j == 0 ? 0.0f : A.cheb_c1[j], A.cheb_c2[j]);
         tm.sync();
-        op_chebc_x(A, D, l, t, T);
+        cur_b = !cur_b;
+    }
+    if (cur_b) {
+        op_copy(t, T, n, xb, xa);
         tm.sync();
     }
 }
 
-// V-cycle with Chebyshev smoothing on the team levels (same structure as
-// team_vcycle; the single-warp tail keeps Gauss-Seidel).
+// The rest of the V-cycle from coarse level l0 (<= kWarpTailCells cells) on
+// one warp with Chebyshev smoothing: cheb_k passes per smoothing instead of
+// the 16 colour passes of two Gauss-Seidel sweeps, coarse_sweeps smoothings
+// on the coarsest level.
+template <int P>
+__device__ void warp_tail_cheb(const KArena& A, const KDesc& D, int l0) {
+    WarpTeam wt;
+    const int t = (int)wt.t(), T = (int)wt.T();
+    const int L = D.nlev;
+    const bool odd = (A.cheb_k & 1) != 0;
+    for (int l = l0; l < L - 1; l++) {
+        team_chebc<P>(A, D, l, wt, true);
+        op_restrictc<P>(A, D, l, t, T);
+        __syncwarp();
+    }
+    team_chebc<P>(A, D, L - 1, wt, true);
+    for (int s = 1; s < A.coarse_sweeps; s++) team_chebc<P>(A, D, L - 1, wt, false);
+    for (int l = L - 2; l >= l0; l--) {
+        float* xa = A.cx + D.lev[l].off;
+        op_prolongc_to(A, D, l, t, T, A.omega_c, xa, odd ? A.cx2 + D.lev[l].off : xa);
+        __syncwarp();
+        team_chebc<P>(A, D, l, wt, false, odd);
+    }
+}
+
+// V-cycle with Chebyshev smoothing on every level (same structure as
+// team_vcycle).
 template <int P, class TeamT>
 __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
     const int t = (int)tm.t(), T = (int)tm.T();
@@ -344,20 +389,23 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
         tm.sync();
     }
     if (D.lev[l0].n <= kWarpTailCells) {
-        if (tm.leader_warp()) warp_tail_vcycle<P>(A, D, l0, A.nu, A.coarse_sweeps, A.omega_c);
+        if (tm.leader_warp()) warp_tail_cheb<P>(A, D, l0);
         tm.sync();
     } else {
         team_chebc<P>(A, D, L - 1, tm, true);
         for (int s = 1; s < A.coarse_sweeps; s++) team_chebc<P>(A, D, L - 1, tm, false);
     }
+    // prolongate into whichever array makes the post-smoothing end in x / z
+    const bool odd = (A.cheb_k & 1) != 0;
     for (int l = l0 - 1; l >= 1; l--) {
-        op_prolongc(A, D, l, t, T, A.omega_c);
+        float* xa = A.cx + D.lev[l].off;
+        op_prolongc_to(A, D, l, t, T, A.omega_c, xa, odd ? A.cx2 + D.lev[l].off : xa);
         tm.sync();
-        team_chebc<P>(A, D, l, tm, false);
+        team_chebc<P>(A, D, l, tm, false, odd);
     }
-    op_prolong0(A, D, t, T, A.omega_c);
+    op_prolong0_to(A, D, t, T, A.omega_c, A.z + D.off, odd ? A.q + D.off : A.z + D.off);
     tm.sync();
-    team_cheb0<P>(A, D, tm, false);
+    team_cheb0<P>(A, D, tm, false, odd);
 }
 
 template <int P, class TeamT>
@@ -382,6 +430,13 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         op_dinv0<P>(A, D, t, T);
         tm.sync();
     }
+    const unsigned long long t_built = globaltimer();
+    unsigned long long t_pc = 0;  // time in V-cycles (the leader's clock, between barriers)
+    auto timed_precondition = [&]() {
+        const unsigned long long a = globaltimer();
+        precondition<P>(A, D, tm);
+        t_pc += globaltimer() - a;
+    };
     double relres = 1.0, bn = 0.0;
     int inner_total = 0, outer = 0;
     bool conv = false;
@@ -397,7 +452,7 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         // inner PCG on A e = r, stopping at ||r_in|| <= eta ||r_out||
         const double eta = fmax(A.eta_min, 0.3 * A.tol / relres);
         const R stop2 = (R)(eta * eta * rr);
-        precondition<P>(A, D, tm);
+        timed_precondition();
         R rz = 0;
         t_dot_rz(A, D, tm, rz);
         rz = tm.sum(rz);
@@ -413,7 +468,7 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
             rri = tm.sum(rri);
             inner_total++;
             if (rri <= stop2 || !(pq > (R)0)) break;
-            precondition<P>(A, D, tm);
+            timed_precondition();
             R rzn = 0;
             t_dot_rz(A, D, tm, rzn);
             rzn = tm.sum(rzn);
@@ -433,6 +488,8 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         D.converged = conv ? 1 : 0;
         D.t_start = t0;
         D.t_end = globaltimer();
+        D.t_setup = t_built - t0;
+        D.t_precond = t_pc;
     }
 }
 

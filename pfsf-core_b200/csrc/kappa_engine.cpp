@@ -141,7 +141,7 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
                  o_cx = take(coarse * 4), o_cb = take(coarse * 4), o_desc = take(sizeof(KDesc) * nisl),
                  o_order = take(sizeof(int) * nisl), o_queue = take(256),
                  o_scr = take(sizeof(float) * kappa::plain_scratch_floats()), o_dinv = take(fine * 4),
-                 o_d0 = take(fine * 4), o_cdd = take(coarse * 4);
+                 o_d0 = take(fine * 4), o_cdd = take(coarse * 4), o_cx2 = take(coarse * 4);
     A->bytes = off;
     if (fault_alloc_after_ >= 0 && alloc_count_ >= fault_alloc_after_) return false;
     if (cudaMalloc(&A->base, A->bytes) != cudaSuccess) {
@@ -178,6 +178,7 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     k.dinv0 = reinterpret_cast<float*>(b + o_dinv);
     k.d0 = reinterpret_cast<float*>(b + o_d0);
     k.cd = reinterpret_cast<float*>(b + o_cdd);
+    k.cx2 = reinterpret_cast<float*>(b + o_cx2);
     k.nisl = nisl;
     k.prec = A->prec;
     if (!CU_OK(cudaMallocHost((void**)&A->hscratch, 256))) return false;
@@ -303,6 +304,8 @@ void Engine::fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_sol
             const double ms = (double)(d.t_end - d.t_start) * 1e-6;
             st.island_ms_sum += ms;
             st.island_ms_max = std::max(st.island_ms_max, ms);
+            st.setup_ms_sum += (double)d.t_setup * 1e-6;
+            st.precond_ms_sum += (double)d.t_precond * 1e-6;
         }
         st.span_ms = t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
     }

@@ -145,19 +145,25 @@ __device__ __forceinline__ void mfor_nb(NB& nb, F f) {
 
 // ---- the marching forms of the fine-level stencil ops
 
-// d = c1 d + c2 D^-1 (r - A' z) on solid voxels (kappa storage P)
+// one whole Chebyshev step out of place (op_cheb0_dz)
 template <int P>
-__device__ void mop_cheb0_d(const KArena& A, const KDesc& D, MarchTile& S, int cta, int ncta, float c1, float c2) {
+__device__ void mop_cheb0_dz(const KArena& A, const KDesc& D, MarchTile& S, int cta, int ncta, const float* zin,
+                             float* zout, float c1, float c2) {
     const Fine F = fine_view(A, D);
     const float* dinv = A.dinv0 + D.off;
     float* d = A.d0 + D.off;
-    march<float>(F, S, cta, ncta, [&](int g) { return F.z[g]; }, [&](int g) { return kpre<P>(F, g); },
+    march<float>(F, S, cta, ncta, [&](int g) { return zin[g]; }, [&](int g) { return kpre<P>(F, g); },
                  [&](int i, float zi, float ki, auto& nb) {
-                     if (F.type[i] != kSolid) return;
+                     if (F.type[i] != kSolid) {
+                         zout[i] = zi;
+                         return;
+                     }
                      float az = 0.0f;
                      mfor_nb<float>(nb, [&](float zj, float kj, float gs) { az += gs * hm(ki, kj) * (zi - zj); });
                      const float upd = c2 * dinv[i] * (F.r[i] - az);
-                     d[i] = c1 == 0.0f ? upd : c1 * d[i] + upd;
+                     const float dn = c1 == 0.0f ? upd : c1 * d[i] + upd;
+                     d[i] = dn;
+                     zout[i] = zi + dn;
                  });
 }
 
@@ -362,13 +368,14 @@ __device__ void vop_pupdate(const KArena& A, const KDesc& D, int t, int T, float
     }
 }
 
-__device__ void vop_cheb0_first(const KArena& A, const KDesc& D, int t, int T, float c2) {
+// zout: F.z or the q array (both island arrays, 128-byte aligned)
+__device__ void vop_cheb0_first(const KArena& A, const KDesc& D, int t, int T, float c2, float* zout) {
     const Fine F = fine_view(A, D);
     const int n4 = F.n >> 2;
     const float4* dv4 = reinterpret_cast<const float4*>(A.dinv0 + D.off);
     const float4* r4 = reinterpret_cast<const float4*>(F.r);
     float4* d4 = reinterpret_cast<float4*>(A.d0 + D.off);
-    float4* z4 = reinterpret_cast<float4*>(F.z);
+    float4* z4 = reinterpret_cast<float4*>(zout);
     for (int j = t; j < n4; j += T) {
         const float4 dv = dv4[j], r = r4[j];
         const float4 v = make_float4(c2 * dv.x * r.x, c2 * dv.y * r.y, c2 * dv.z * r.z, c2 * dv.w * r.w);
@@ -380,30 +387,16 @@ __device__ void vop_cheb0_first(const KArena& A, const KDesc& D, int t, int T, f
     for (int i = 4 * n4 + t; i < F.n; i += T) {
         const float v = c2 * dinv[i] * F.r[i];
         d[i] = v;
-        F.z[i] = v;
+        zout[i] = v;
     }
 }
 
-// z += d on solid voxels (d is 0 off solid voxels after every d-pass)
-__device__ void vop_cheb0_z(const KArena& A, const KDesc& D, int t, int T) {
-    const Fine F = fine_view(A, D);
-    const int n4 = F.n >> 2;
-    const float4* d4 = reinterpret_cast<const float4*>(A.d0 + D.off);
-    const uchar4* t4 = reinterpret_cast<const uchar4*>(F.type);
-    float4* z4 = reinterpret_cast<float4*>(F.z);
-    for (int j = t; j < n4; j += T) {
-        const uchar4 ty = t4[j];
-        const float4 d = d4[j];
-        float4 z = z4[j];
-        if (ty.x == kSolid) z.x += d.x;
-        if (ty.y == kSolid) z.y += d.y;
-        if (ty.z == kSolid) z.z += d.z;
-        if (ty.w == kSolid) z.w += d.w;
-        z4[j] = z;
-    }
-    const float* d = A.d0 + D.off;
-    for (int i = 4 * n4 + t; i < F.n; i += T)
-        if (F.type[i] == kSolid) F.z[i] += d[i];
+__device__ void vop_copy(int t, int T, int n, const float* src, float* dst) {
+    const int n4 = n >> 2;
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int j = t; j < n4; j += T) d4[j] = s4[j];
+    for (int i = 4 * n4 + t; i < n; i += T) dst[i] = src[i];
 }
 
 __device__ void vop_accumulate(const KArena& A, const KDesc& D, int t, int T) {

@@ -442,6 +442,20 @@ __device__ void op_prolongc(const KArena& A, const KDesc& D, int l, int t, int T
         F.x[f] += omega * C.x[c];
     }
 }
+// xout = xin + omega * x_{l+1}[parent] on active cells of level l, xout = xin elsewhere
+__device__ void op_prolongc_to(const KArena& A, const KDesc& D, int l, int t, int T, float omega, const float* xin,
+                               float* xout) {
+    const Coarse F = coarse_view(A, D, l);
+    const Coarse C = coarse_view(A, D, l + 1);
+    for (int f = t; f < F.n; f += T) {
+        float v = xin[f];
+        if (F.diag[f] > 0.0f) {
+            const Pos p = decode((unsigned)f, (unsigned)F.lx, (unsigned)F.ly);
+            v += omega * C.x[(p.x >> 1) + C.lx * ((p.y >> 1) + C.ly * (p.z >> 1))];
+        }
+        xout[f] = v;
+    }
+}
 
 // ---- Chebyshev smoothing (polynomial in D^-1 A' on [lambda_max/10, lambda_max],
 // lambda_max = 2, the Gershgorin bound of a weakly diagonally dominant
@@ -462,73 +476,97 @@ __device__ void op_dinv0(const KArena& A, const KDesc& D, int t, int T) {
         dinv[i] = d > 0.0f ? 1.0f / d : 0.0f;
     }
 }
-// first pre-smoothing step from z = 0: d = c2 D^-1 r, z = d
-__device__ void op_cheb0_first(const KArena& A, const KDesc& D, int t, int T, float c2) {
+// first pre-smoothing step from z = 0: d = c2 D^-1 r, zout = d (dinv is 0 off
+// solid voxels, so zout is too)
+__device__ void op_cheb0_first(const KArena& A, const KDesc& D, int t, int T, float c2, float* zout) {
     const Fine F = fine_view(A, D);
     const float* dinv = A.dinv0 + D.off;
     float* d = A.d0 + D.off;
     for (int i = t; i < F.n; i += T) {
         const float v = c2 * dinv[i] * F.r[i];
         d[i] = v;
-        F.z[i] = v;
+        zout[i] = v;
     }
 }
-// d = c1 d + c2 D^-1 (r - A' z)   (c1 == 0: d is not read)
+// One whole Chebyshev step in one pass, out of place:
+//   d = c1 d + c2 D^-1 (r - A' zin),  zout = zin + d     (solid voxels; zout = zin elsewhere)
+// (zin and zout are different arrays, so the pass reads nothing it writes)
 template <int P>
-__device__ void op_cheb0_d(const KArena& A, const KDesc& D, int t, int T, float c1, float c2) {
+__device__ void op_cheb0_dz(const KArena& A, const KDesc& D, int t, int T, const float* zin, float* zout, float c1,
+                            float c2) {
     const Fine F = fine_view(A, D);
     const float* dinv = A.dinv0 + D.off;
     float* d = A.d0 + D.off;
     for (int i = t; i < F.n; i += T) {
-        if (F.type[i] != kSolid) continue;
+        const float zi = zin[i];
+        if (F.type[i] != kSolid) {
+            zout[i] = zi;
+            continue;
+        }
         const Pos p = decode((unsigned)i, (unsigned)F.lx, (unsigned)F.ly);
-        const float ki = kpre<P>(F, i), zi = F.z[i];
+        const float ki = kpre<P>(F, i);
         float az = 0.0f;
         for_nb(p, F.lx, F.ly, F.lz, [&](int, int, int, int dj, float gs) {
-            az += gs * hm(ki, kpre<P>(F, i + dj)) * (zi - F.z[i + dj]);
+            az += gs * hm(ki, kpre<P>(F, i + dj)) * (zi - zin[i + dj]);
         });
         const float upd = c2 * dinv[i] * (F.r[i] - az);
-        d[i] = c1 == 0.0f ? upd : c1 * d[i] + upd;
+        const float dn = c1 == 0.0f ? upd : c1 * d[i] + upd;
+        d[i] = dn;
+        zout[i] = zi + dn;
     }
 }
-__device__ void op_cheb0_z(const KArena& A, const KDesc& D, int t, int T) {
+// zout = zin + omega * x1[aggregate(i)] on solid voxels, zout = zin elsewhere
+__device__ void op_prolong0_to(const KArena& A, const KDesc& D, int t, int T, float omega, const float* zin,
+                               float* zout) {
     const Fine F = fine_view(A, D);
-    const float* d = A.d0 + D.off;
-    for (int i = t; i < F.n; i += T)
-        if (F.type[i] == kSolid) F.z[i] += d[i];
+    const Coarse C = coarse_view(A, D, 1);
+    for (int i = t; i < F.n; i += T) {
+        float v = zin[i];
+        if (F.type[i] == kSolid) {
+            const Pos p = decode((unsigned)i, (unsigned)F.lx, (unsigned)F.ly);
+            v += omega * C.x[(p.x >> 1) + C.lx * ((p.y >> 1) + C.ly * (p.z >> 1))];
+        }
+        zout[i] = v;
+    }
+}
+__device__ void op_copy(int t, int T, int n, const float* src, float* dst) {
+    for (int i = t; i < n; i += T) dst[i] = src[i];
 }
 // coarse level l: first step from x = 0
-__device__ void op_chebc_first(const KArena& A, const KDesc& D, int l, int t, int T, float c2) {
+// coarse level l: first step from x = 0 into xout (the level's x or x2 array)
+__device__ void op_chebc_first(const KArena& A, const KDesc& D, int l, int t, int T, float c2, float* xout) {
     const Coarse L = coarse_view(A, D, l);
     float* d = A.cd + D.lev[l].off;
     for (int c = t; c < L.n; c += T) {
         const float dg = L.diag[c];
         const float v = dg > 0.0f ? c2 * L.b[c] / dg : 0.0f;
         d[c] = v;
-        L.x[c] = v;
+        xout[c] = v;
     }
 }
+// one whole coarse Chebyshev step out of place:
+//   d = c1 d + c2 (b - A_c xin) / diag,  xout = xin + d   (active cells; xout = xin elsewhere)
 template <int P>
-__device__ void op_chebc_d(const KArena& A, const KDesc& D, int l, int t, int T, float c1, float c2) {
+__device__ void op_chebc_dx(const KArena& A, const KDesc& D, int l, int t, int T, const float* xin, float* xout,
+                            float c1, float c2) {
     const Coarse L = coarse_view(A, D, l);
     float* d = A.cd + D.lev[l].off;
     for (int c = t; c < L.n; c += T) {
-        const float dg = L.diag[c];
-        if (!(dg > 0.0f)) continue;
+        const float dg = L.diag[c], xc = xin[c];
+        if (!(dg > 0.0f)) {
+            xout[c] = xc;
+            continue;
+        }
         const Pos p = decode((unsigned)c, (unsigned)L.lx, (unsigned)L.ly);
         float s = 0.0f;
         for_nb(p, L.lx, L.ly, L.lz, [&](int dx, int dy, int dz, int dj, float) {
-            s += cget<P>(L, nbk(dx, dy, dz), c) * L.x[c + dj];
+            s += cget<P>(L, nbk(dx, dy, dz), c) * xin[c + dj];
         });
-        const float upd = c2 * (L.b[c] - (dg * L.x[c] - s)) / dg;
-        d[c] = c1 == 0.0f ? upd : c1 * d[c] + upd;
+        const float upd = c2 * (L.b[c] - (dg * xc - s)) / dg;
+        const float dn = c1 == 0.0f ? upd : c1 * d[c] + upd;
+        d[c] = dn;
+        xout[c] = xc + dn;
     }
-}
-__device__ void op_chebc_x(const KArena& A, const KDesc& D, int l, int t, int T) {
-    const Coarse L = coarse_view(A, D, l);
-    const float* d = A.cd + D.lev[l].off;
-    for (int c = t; c < L.n; c += T)
-        if (L.diag[c] > 0.0f) L.x[c] += d[c];
 }
 
 // One warp runs the V-cycle from coarse level l0 down to the coarsest level

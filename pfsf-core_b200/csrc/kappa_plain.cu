@@ -148,11 +148,13 @@ void launch_to_f32(cudaStream_t s, const KArena& a, int64_t n) {
     k_to_f32<<<(unsigned)ceil_div64(n, 256), 256, 0, s>>>(a.x64, a.e, n);
 }
 
+// Coarsen by 2 per axis until a level has at most 64 cells (or a side of 2,
+// or kMaxLevels levels).
 int plan_levels(int lx, int ly, int lz, KLevel* lev) {
     int nlev = 1;
     int x = lx, y = ly, z = lz;
     lev[0] = KLevel{lx, ly, lz, 0, 0, (int64_t)lx * ly * lz};
-    while (nlev < kMaxLevels && std::max(x, std::max(y, z)) > 2) {
+    while (nlev < kMaxLevels && std::max(x, std::max(y, z)) > 2 && (int64_t)x * y * z > 64) {
         x = (x + 1) / 2; y = (y + 1) / 2; z = (z + 1) / 2;
         lev[nlev] = KLevel{x, y, z, 0, 0, (int64_t)x * y * z};
         nlev++;

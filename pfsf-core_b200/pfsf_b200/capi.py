@@ -86,7 +86,7 @@ class SolveStats(C.Structure):
                 ("upload_ms", C.c_float), ("readback_ms", C.c_float), ("kernel_launches", C.c_int32),
                 ("inner_iterations_total", C.c_int64), ("algorithmic_bytes", C.c_double),
                 ("active_voxels", C.c_int64), ("island_ms_sum", C.c_double), ("island_ms_max", C.c_double),
-                ("span_ms", C.c_double)]
+                ("span_ms", C.c_double), ("setup_ms_sum", C.c_double), ("precond_ms_sum", C.c_double)]
 
 
 _lib = None
