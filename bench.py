@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--islands", type=int, default=4096)
     ap.add_argument("--target-active", type=float, default=6.0e7)
     ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--island-report", default="",
+                    help="write one JSON line per island of the last timed solve (team, iterations, times)")
     ap.add_argument("--precision", choices=["bf16", "fp16", "fp32"], default="bf16")
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -90,6 +92,22 @@ def make_workload(args, rank):
         return isls, meta
     return synth.batch(args.islands, seed=7 + 1000 * rank, target_active=args.target_active,
                        workers=min(32, os.cpu_count() or 1))
+
+
+def write_island_report(path, eng, ids, isls):
+    from pfsf_b200.capi import IslandReport
+    with open(path, "w") as f:
+        for iid, isl in zip(ids, isls):
+            rc, r = eng.island_report(int(iid))
+            if rc != 0:
+                raise RuntimeError(f"pfsf_island_solve_report({iid}) returned {rc}")
+            f.write(json.dumps({"id": int(iid), "dims": [r.lx, r.ly, r.lz], "n": int(isl.n),
+                                "active": int(isl.n_active), "levels": r.levels,
+                                "team": IslandReport.TEAMS.get(r.team, str(r.team)), "team_ctas": r.team_ctas,
+                                "inner": r.inner_iterations, "outer": r.outer_iterations,
+                                "converged": r.converged, "rel_residual": r.rel_residual,
+                                "solve_ms": r.solve_ms, "setup_ms": r.setup_ms,
+                                "precond_ms": r.precond_ms}) + "\n")
 
 
 def stratified(isls, k):
@@ -281,6 +299,8 @@ def run_ours(args):
         torch.cuda.synchronize()
     launches = eng.launches() - launches0
     ms = ev0.elapsed_time(ev1) / args.steps
+    if args.island_report and rank == 0:
+        write_island_report(args.island_report, eng, ids, isls)
     if ws > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -383,7 +403,10 @@ def run_ours(args):
             "schedule": {"island_ms_sum": stats[-1].island_ms_sum, "island_ms_max": stats[-1].island_ms_max,
                          "span_ms": stats[-1].span_ms, "setup_ms_sum": stats[-1].setup_ms_sum,
                          "precond_ms_sum": stats[-1].precond_ms_sum,
-                         "cluster": os.environ.get("PFSF_CLUSTER", "16"),
+                         "vcycle_ms_sum": {"fine": stats[-1].vcycle_fine_ms_sum,
+                                           "coarse": stats[-1].vcycle_coarse_ms_sum,
+                                           "tail": stats[-1].vcycle_tail_ms_sum},
+                         "cluster": os.environ.get("PFSF_CLUSTER", "8"),
                          "cluster_min_voxels": os.environ.get("PFSF_CLUSTER_MIN_VOXELS", "131072"),
                          "warp_max_voxels": os.environ.get("PFSF_WARP_MAX_VOXELS", "0"),
                          "smoother": os.environ.get("PFSF_SMOOTHER", "chebyshev(batched)"), "cheb_k": os.environ.get("PFSF_CHEB_K", "3")},

@@ -66,6 +66,9 @@ typedef struct pfsf_solve_stats {
     double span_ms;                 /* batched mode: first island start to last island end */
     double setup_ms_sum;            /* batched mode: sum over islands of the hierarchy build */
     double precond_ms_sum;          /* batched mode: sum over islands of the time in V-cycles */
+    double vcycle_fine_ms_sum;      /* ... of which fine-level passes */
+    double vcycle_coarse_ms_sum;    /* ... coarse levels smoothed by the whole team */
+    double vcycle_tail_ms_sum;      /* ... the coarsest levels (single warp or team) */
 } pfsf_solve_stats;
 
 /* Registers the kappa-form inputs of an island created by pfsf_add_island.
@@ -100,6 +103,34 @@ PFSF_API pfsf_result pfsf_solve_to_tolerance(pfsf_engine engine, const int32_t* 
 PFSF_API pfsf_result pfsf_tick_tolerance(pfsf_engine engine, const int32_t* island_ids, int32_t count,
                                          int64_t epoch, void* failure_addr, int64_t failure_bytes, double rel_tol,
                                          int32_t max_iter, pfsf_solve_stats* out);
+
+/* No counterpart in the reference ABI.  Convergence record of one island in
+ * the last forward tolerance solve of the current island set (an adjoint
+ * solve leaves it in place).  INVALID_ARG before any solve of the set. */
+typedef enum pfsf_island_team {
+    PFSF_TEAM_PLAIN = 0,   /* plain mode: one kernel per operation */
+    PFSF_TEAM_GRID = 1,    /* the whole GPU (cooperative launch) */
+    PFSF_TEAM_CLUSTER = 2, /* one thread-block cluster */
+    PFSF_TEAM_CTA = 3,     /* one CTA */
+    PFSF_TEAM_WARP = 4     /* one warp */
+} pfsf_island_team;
+
+typedef struct pfsf_island_report {
+    int32_t struct_bytes;
+    int32_t lx, ly, lz;
+    int32_t levels;            /* hierarchy levels including the fine level */
+    int32_t inner_iterations;  /* inner PCG iterations over all outer steps */
+    int32_t outer_iterations;  /* FP64 residual refinements */
+    int32_t converged;         /* 1 when rel_residual <= the requested tolerance */
+    int32_t team;              /* pfsf_island_team */
+    int32_t team_ctas;         /* CTAs of the team (0 for a warp or plain mode) */
+    double rel_residual;       /* final ||s - A phi|| / ||s|| (FP64) */
+    double solve_ms;           /* batched mode: the island's solve time */
+    double setup_ms;           /* batched mode: hierarchy build */
+    double precond_ms;         /* batched mode: time in V-cycles */
+} pfsf_island_report;
+
+PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine engine, int32_t island_id, pfsf_island_report* out);
 
 /* Copies the FP64 solution accumulator of the last tolerance solve of an
  * island (count = min(N, capacity) values).  The FP32 phi written back by

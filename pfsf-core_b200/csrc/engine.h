@@ -151,6 +151,7 @@ public:
     pfsf_result solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter, uint32_t flags,
                                    pfsf_solve_stats* out);
     pfsf_result read_solution64(int32_t id, double* out, int64_t cap, int64_t* count);
+    pfsf_result island_report(int32_t id, pfsf_island_report* out) const;
     pfsf_result tick_tolerance(const int32_t* ids, int32_t count, void* fail_addr, int64_t fail_bytes, double tol,
                                int32_t max_iter, pfsf_solve_stats* out);
     pfsf_result register_adjoint(int32_t id, const pfsf_island_adjoint_buffers* b);
@@ -217,7 +218,7 @@ private:
     int num_sms_ = 148;
     int64_t grid_min_voxels_ = 1 << 21;    // PFSF_GRID_MIN_VOXELS: whole-GPU tier
     int64_t cluster_min_voxels_ = 131072;  // PFSF_CLUSTER_MIN_VOXELS
-    int cluster_size_ = 16;               // PFSF_CLUSTER (16, 8 or 1)
+    int cluster_size_ = 8;                // PFSF_CLUSTER (16, 8 or 1)
     int64_t warp_max_voxels_ = 0;         // PFSF_WARP_MAX_VOXELS (0: no warp tier)
     int smoother_ = -1;                   // PFSF_SMOOTHER (-1: mode default)
     int cheb_k_ = 3;                      // PFSF_CHEB_K

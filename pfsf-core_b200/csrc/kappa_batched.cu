@@ -53,7 +53,9 @@ struct SharedScratch {
 // Team = one CTA.
 struct CtaTeam {
     static constexpr bool kMarch = false;  // fine passes by the generic per-voxel ops
+    static constexpr int kKind = 3;        // PFSF_TEAM_CTA
     SharedScratch* sh;
+    __device__ int ctas() const { return 1; }
     __device__ int64_t t() const { return threadIdx.x; }
     __device__ int64_t T() const { return blockDim.x; }
     __device__ bool leader() const { return threadIdx.x == 0; }
@@ -66,6 +68,8 @@ struct CtaTeam {
 // Team = one warp (small islands): warp barriers only, shuffle reductions.
 struct WarpTeam {
     static constexpr bool kMarch = false;
+    static constexpr int kKind = 4;  // PFSF_TEAM_WARP
+    __device__ int ctas() const { return 0; }
     __device__ int64_t t() const { return threadIdx.x & 31; }
     __device__ int64_t T() const { return 32; }
     __device__ bool leader() const { return (threadIdx.x & 31) == 0; }
@@ -82,8 +86,10 @@ struct WarpTeam {
 template <int C>
 struct ClusterTeam {
     static constexpr bool kMarch = false;
+    static constexpr int kKind = 2;  // PFSF_TEAM_CLUSTER
     SharedScratch* sh;
     int parity = 0;
+    __device__ int ctas() const { return C; }
     __device__ int64_t t() const { return (int64_t)cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
     __device__ int64_t T() const { return (int64_t)C * blockDim.x; }
     __device__ bool leader() const { return cg::this_cluster().block_rank() == 0 && threadIdx.x == 0; }
@@ -131,6 +137,7 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 
 struct GridTeam {
     static constexpr bool kMarch = true;  // fine passes by plane marching (kappa_march.cuh)
+    static constexpr int kKind = 1;       // PFSF_TEAM_GRID
     SharedScratch* sh;
     unsigned* count;  // arrivals at the current barrier
     unsigned* gen;    // barrier generation
@@ -140,6 +147,7 @@ struct GridTeam {
     int parity = 0;
     __device__ int cta() const { return blockIdx.x; }
     __device__ int ncta() const { return gridDim.x; }
+    __device__ int ctas() const { return gridDim.x; }
     __device__ int64_t t() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
     __device__ int64_t T() const { return (int64_t)gridDim.x * blockDim.x; }
     __device__ bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
@@ -368,14 +376,21 @@ __device__ void warp_tail_cheb(const KArena& A, const KDesc& D, int l0) {
 }
 
 // V-cycle with Chebyshev smoothing on every level (same structure as
-// team_vcycle).
+// team_vcycle).  Time spent in each part (the leader's clock, between
+// barriers) accumulates into vt.
+struct VTimes {
+    unsigned long long fine = 0, coarse = 0, tail = 0;
+};
+
 template <int P, class TeamT>
-__device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
+__device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTimes& vt) {
     const int t = (int)tm.t(), T = (int)tm.T();
     const int L = D.nlev;
+    unsigned long long c0 = globaltimer();
     if (L <= 1) {
         team_cheb0<P>(A, D, tm, true);
         team_cheb0<P>(A, D, tm, false);
+        vt.fine += globaltimer() - c0;
         return;
     }
     int l0 = 1;
@@ -383,11 +398,15 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
     team_cheb0<P>(A, D, tm, true);
     t_restrict0<P>(A, D, tm);
     tm.sync();
+    unsigned long long c1 = globaltimer();
+    vt.fine += c1 - c0;
     for (int l = 1; l < l0; l++) {
         team_chebc<P>(A, D, l, tm, true);
         op_restrictc<P>(A, D, l, t, T);
         tm.sync();
     }
+    c0 = globaltimer();
+    vt.coarse += c0 - c1;
     if (D.lev[l0].n <= kWarpTailCells) {
         if (tm.leader_warp()) warp_tail_cheb<P>(A, D, l0);
         tm.sync();
@@ -395,6 +414,8 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
         team_chebc<P>(A, D, L - 1, tm, true);
         for (int s = 1; s < A.coarse_sweeps; s++) team_chebc<P>(A, D, L - 1, tm, false);
     }
+    c1 = globaltimer();
+    vt.tail += c1 - c0;
     // prolongate into whichever array makes the post-smoothing end in x / z
     const bool odd = (A.cheb_k & 1) != 0;
     for (int l = l0 - 1; l >= 1; l--) {
@@ -403,14 +424,17 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
         tm.sync();
         team_chebc<P>(A, D, l, tm, false, odd);
     }
+    c0 = globaltimer();
+    vt.coarse += c0 - c1;
     op_prolong0_to(A, D, t, T, A.omega_c, A.z + D.off, odd ? A.q + D.off : A.z + D.off);
     tm.sync();
     team_cheb0<P>(A, D, tm, false, odd);
+    vt.fine += globaltimer() - c0;
 }
 
 template <int P, class TeamT>
-__device__ __forceinline__ void precondition(const KArena& A, const KDesc& D, TeamT& tm) {
-    if (A.smoother == 1) team_vcycle_cheb<P>(A, D, tm);
+__device__ __forceinline__ void precondition(const KArena& A, const KDesc& D, TeamT& tm, VTimes& vt) {
+    if (A.smoother == 1) team_vcycle_cheb<P>(A, D, tm, vt);
     else team_vcycle<P>(A, D, tm);
 }
 
@@ -432,9 +456,10 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
     }
     const unsigned long long t_built = globaltimer();
     unsigned long long t_pc = 0;  // time in V-cycles (the leader's clock, between barriers)
+    VTimes vt;
     auto timed_precondition = [&]() {
         const unsigned long long a = globaltimer();
-        precondition<P>(A, D, tm);
+        precondition<P>(A, D, tm, vt);
         t_pc += globaltimer() - a;
     };
     double relres = 1.0, bn = 0.0;
@@ -490,6 +515,11 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         D.t_end = globaltimer();
         D.t_setup = t_built - t0;
         D.t_precond = t_pc;
+        D.t_vfine = vt.fine;
+        D.t_vcoarse = vt.coarse;
+        D.t_vtail = vt.tail;
+        D.team = TeamT::kKind;
+        D.team_ctas = tm.ctas();
     }
 }
 

@@ -306,6 +306,9 @@ void Engine::fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_sol
             st.island_ms_max = std::max(st.island_ms_max, ms);
             st.setup_ms_sum += (double)d.t_setup * 1e-6;
             st.precond_ms_sum += (double)d.t_precond * 1e-6;
+            st.vcycle_fine_ms_sum += (double)d.t_vfine * 1e-6;
+            st.vcycle_coarse_ms_sum += (double)d.t_vcoarse * 1e-6;
+            st.vcycle_tail_ms_sum += (double)d.t_vtail * 1e-6;
         }
         st.span_ms = t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
     }
@@ -480,6 +483,31 @@ pfsf_result Engine::adjoint_to_tolerance(const int32_t* ids, int32_t count, doub
     st.readback_ms = t_rb;
     st.kernel_launches = (int32_t)std::min<int64_t>(nl, INT32_MAX);
     if (out) *out = st;
+    return PFSF_OK;
+}
+
+pfsf_result Engine::island_report(int32_t id, pfsf_island_report* out) const {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (!out || !arena_ || !arena_->solved) return PFSF_ERROR_INVALID_ARG;
+    auto it = std::find(arena_->ids.begin(), arena_->ids.end(), id);
+    if (it == arena_->ids.end()) return PFSF_ERROR_INVALID_ARG;
+    const KDesc& d = arena_->desc[it - arena_->ids.begin()];
+    pfsf_island_report r{};
+    r.struct_bytes = (int32_t)sizeof(r);
+    r.lx = d.lx; r.ly = d.ly; r.lz = d.lz;
+    r.levels = d.nlev;
+    r.inner_iterations = d.inner_iters;
+    r.outer_iterations = d.outer_iters;
+    r.converged = d.converged;
+    r.team = d.team;
+    r.team_ctas = d.team_ctas;
+    r.rel_residual = d.relres;
+    if (d.team != PFSF_TEAM_PLAIN) {
+        r.solve_ms = (double)(d.t_end - d.t_start) * 1e-6;
+        r.setup_ms = (double)d.t_setup * 1e-6;
+        r.precond_ms = (double)d.t_precond * 1e-6;
+    }
+    *out = r;
     return PFSF_OK;
 }
 

@@ -176,6 +176,11 @@ PFSF_API pfsf_result pfsf_tick_tolerance(pfsf_engine e, const int32_t* ids, int3
     return g ? g->tick_tolerance(ids, count, fail_addr, fail_bytes, rel_tol, max_iter, out) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine e, int32_t id, pfsf_island_report* out) {
+    Engine* g = E(e);
+    return g ? g->island_report(id, out) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine e, int32_t id, double* out, int64_t cap, int64_t* count) {
     Engine* g = E(e);
     return g ? g->read_solution64(id, out, cap, count) : PFSF_ERROR_INVALID_ARG;

@@ -86,7 +86,18 @@ class SolveStats(C.Structure):
                 ("upload_ms", C.c_float), ("readback_ms", C.c_float), ("kernel_launches", C.c_int32),
                 ("inner_iterations_total", C.c_int64), ("algorithmic_bytes", C.c_double),
                 ("active_voxels", C.c_int64), ("island_ms_sum", C.c_double), ("island_ms_max", C.c_double),
-                ("span_ms", C.c_double), ("setup_ms_sum", C.c_double), ("precond_ms_sum", C.c_double)]
+                ("span_ms", C.c_double), ("setup_ms_sum", C.c_double), ("precond_ms_sum", C.c_double),
+                ("vcycle_fine_ms_sum", C.c_double), ("vcycle_coarse_ms_sum", C.c_double),
+                ("vcycle_tail_ms_sum", C.c_double)]
+
+
+class IslandReport(C.Structure):
+    TEAMS = {0: "plain", 1: "grid", 2: "cluster", 3: "cta", 4: "warp"}
+    _fields_ = [("struct_bytes", C.c_int32), ("lx", C.c_int32), ("ly", C.c_int32), ("lz", C.c_int32),
+                ("levels", C.c_int32), ("inner_iterations", C.c_int32), ("outer_iterations", C.c_int32),
+                ("converged", C.c_int32), ("team", C.c_int32), ("team_ctas", C.c_int32),
+                ("rel_residual", C.c_double), ("solve_ms", C.c_double), ("setup_ms", C.c_double),
+                ("precond_ms", C.c_double)]
 
 
 _lib = None
@@ -131,6 +142,7 @@ def load():
         "pfsf_solve_to_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_int32, C.c_uint32,
                                      C.POINTER(SolveStats)], C.c_int),
         "pfsf_read_solution64": ([E, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "pfsf_island_solve_report": ([E, C.c_int32, C.c_void_p], C.c_int),
         "pfsf_tick_tolerance": ([E, C.POINTER(C.c_int32), C.c_int32, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
                                  C.c_int32, C.POINTER(SolveStats)], C.c_int),
         "pfsf_label_components": ([E, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
@@ -261,6 +273,11 @@ class Engine:
         rc = self.L.pfsf_adjoint_to_tolerance(self.h, ids.ctypes.data_as(C.POINTER(C.c_int32)), ids.size, tol,
                                               max_iter, flags, C.byref(st))
         return rc, st
+
+    def island_report(self, iid):
+        r = IslandReport()
+        rc = self.L.pfsf_island_solve_report(self.h, iid, C.byref(r))
+        return rc, r
 
     def read_solution64(self, iid, n):
         out = np.zeros(n, np.float64)

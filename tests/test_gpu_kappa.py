@@ -80,8 +80,18 @@ def test_batched_uneven_islands(eng):
     assert rc == capi.PFSF_OK
     assert st.islands_converged == len(isls)
     assert st.max_rel_residual <= TOL
+    inner = 0
     for isl, (iid, host) in zip(isls, reg):
         _check(eng, isl, iid, host)
+        rc, r = eng.island_report(iid)
+        assert rc == capi.PFSF_OK
+        assert (r.lx, r.ly, r.lz) == isl.dims and r.converged == 1 and r.rel_residual <= TOL
+        assert capi.IslandReport.TEAMS[r.team] in ("cta", "warp", "cluster") and r.solve_ms > 0
+        assert r.setup_ms + r.precond_ms <= r.solve_ms
+        inner += r.inner_iterations
+    assert inner == st.inner_iterations_total
+    rc, _ = eng.island_report(987654)
+    assert rc == capi.PFSF_ERROR_INVALID_ARG
 
 
 def test_warm_start_resolve_is_immediate(eng):
