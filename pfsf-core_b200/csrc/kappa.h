@@ -12,6 +12,27 @@ namespace pfsf_b200 {
 // smoothed by the whole team.
 constexpr int kMaxLevels = 5;
 
+// Fine-level stencil passes of CTA-granular teams march over plane tiles of
+// tx x ty columns (kappa_flat.cuh); a tile plane with its one-voxel halo has
+// at most kFlatCap cells, one CTA of kFlatThreads threads stages it in
+// shared memory.  tx and ty are even unless they cover the whole island
+// side, so every 2 x 2 x 2 aggregate of the next level lies in one tile.
+constexpr int kFlatCap = 2048;
+constexpr int kFlatThreads = 512;
+constexpr int kFlatMaxTX = 126;
+constexpr int kFlatZ = 16;  // planes per work item when several CTAs share an island
+__host__ __device__ inline void flat_tile(int lx, int ly, int& tx, int& ty) {
+    tx = lx <= kFlatMaxTX ? lx : kFlatMaxTX;
+    ty = (kFlatCap / (tx + 2) - 2) & ~1;
+    if (ty >= ly) ty = ly;
+}
+// entries of an island's per-(tile, plane) solid-list offset table
+__host__ __device__ inline int64_t flat_starts(int lx, int ly, int lz) {
+    int tx, ty;
+    flat_tile(lx, ly, tx, ty);
+    return (int64_t)((lx + tx - 1) / tx) * ((ly + ty - 1) / ty) * lz + 1;
+}
+
 struct KLevel {
     int lx, ly, lz;
     int pad;
@@ -24,6 +45,7 @@ struct KDesc {
     int lx, ly, lz, nlev;
     int64_t off;  // first voxel in the fine arrays
     int64_t n;
+    int64_t soff;  // first entry of the island's solid-list offset table
     KLevel lev[kMaxLevels];  // lev[0] unused (fine level), 1..nlev-1 coarse
     // results
     double relres;
@@ -70,6 +92,11 @@ struct KArena {
     int smoother;          // 0 symmetric 8-colour Gauss-Seidel, 1 Chebyshev
     int cheb_k;            // polynomial degree (stencil passes per smoothing)
     float cheb_c1[4], cheb_c2[4];
+    // per island: solid voxels of each (tile, plane) as packed tile columns
+    // (cx | cy << 16), island-relative at desc.off, and the table of list
+    // offsets per (tile, plane) at desc.soff (built by each solve)
+    uint32_t* flist;
+    int* fstart;
 };
 
 struct KappaState {

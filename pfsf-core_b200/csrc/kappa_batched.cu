@@ -22,7 +22,7 @@
 #include <algorithm>
 #include <cstdio>
 
-#include "kappa_march.cuh"
+#include "kappa_flat.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -35,6 +35,7 @@ namespace {
 // registers per thread (measured: 256 x 2 with 128 registers took 1.8x longer).
 constexpr int kBatchedThreads = 512;
 constexpr int kBatchedMinBlocks = 2;
+static_assert(kBatchedThreads == kFlatThreads, "the tile marching passes assume one CTA of kFlatThreads");
 
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
@@ -52,9 +53,12 @@ struct SharedScratch {
 
 // Team = one CTA.
 struct CtaTeam {
-    static constexpr bool kMarch = false;  // fine passes by the generic per-voxel ops
-    static constexpr int kKind = 3;        // PFSF_TEAM_CTA
+    static constexpr bool kFlat = true;  // fine passes by tile marching (kappa_flat.cuh)
+    static constexpr int kKind = 3;      // PFSF_TEAM_CTA
     SharedScratch* sh;
+    FlatSmem* fs;
+    __device__ int cta() const { return 0; }
+    __device__ int ncta() const { return 1; }
     __device__ int ctas() const { return 1; }
     __device__ int64_t t() const { return threadIdx.x; }
     __device__ int64_t T() const { return blockDim.x; }
@@ -67,7 +71,7 @@ struct CtaTeam {
 
 // Team = one warp (small islands): warp barriers only, shuffle reductions.
 struct WarpTeam {
-    static constexpr bool kMarch = false;
+    static constexpr bool kFlat = false;  // fine passes by the generic per-voxel ops
     static constexpr int kKind = 4;  // PFSF_TEAM_WARP
     __device__ int ctas() const { return 0; }
     __device__ int64_t t() const { return threadIdx.x & 31; }
@@ -85,10 +89,13 @@ struct WarpTeam {
 // rank order by every CTA -- identical, deterministic results everywhere.
 template <int C>
 struct ClusterTeam {
-    static constexpr bool kMarch = false;
+    static constexpr bool kFlat = true;
     static constexpr int kKind = 2;  // PFSF_TEAM_CLUSTER
     SharedScratch* sh;
+    FlatSmem* fs;
     int parity = 0;
+    __device__ int cta() const { return (int)cg::this_cluster().block_rank(); }
+    __device__ int ncta() const { return C; }
     __device__ int ctas() const { return C; }
     __device__ int64_t t() const { return (int64_t)cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
     __device__ int64_t T() const { return (int64_t)C * blockDim.x; }
@@ -136,14 +143,14 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 }
 
 struct GridTeam {
-    static constexpr bool kMarch = true;  // fine passes by plane marching (kappa_march.cuh)
-    static constexpr int kKind = 1;       // PFSF_TEAM_GRID
+    static constexpr bool kFlat = true;
+    static constexpr int kKind = 1;  // PFSF_TEAM_GRID
     SharedScratch* sh;
     unsigned* count;  // arrivals at the current barrier
     unsigned* gen;    // barrier generation
     int* err;         // set on a timed-out wait
     double* slots;    // [2][kGridMaxBlocks] CTA partials
-    MarchTile* mt;
+    FlatSmem* fs;
     int parity = 0;
     __device__ int cta() const { return blockIdx.x; }
     __device__ int ncta() const { return gridDim.x; }
@@ -196,57 +203,57 @@ struct GridTeam {
     __device__ float sum(float v) { return gsum<float>(v, sh->shf); }
 };
 
-// Fine-level passes: plane marching / four-wide streaming for marching teams,
-// the generic per-voxel ops otherwise.
+// Fine-level passes: tile marching / four-wide streaming for CTA-granular
+// teams, the generic per-voxel ops for warp teams.  The FP64 outer residual
+// (a few passes per solve) always takes the generic op.
 template <class TeamT>
 __device__ __forceinline__ void t_outer_residual(const KArena& A, const KDesc& D, TeamT& tm, double& rr, double& bb) {
-    if constexpr (TeamT::kMarch) mop_outer_residual(A, D, *tm.mt, tm.cta(), tm.ncta(), rr, bb);
-    else op_outer_residual(A, D, (int)tm.t(), (int)tm.T(), rr, bb);
+    op_outer_residual(A, D, (int)tm.t(), (int)tm.T(), rr, bb);
 }
 template <class R, class TeamT>
 __device__ __forceinline__ void t_matvec(const KArena& A, const KDesc& D, TeamT& tm, R& pq) {
-    if constexpr (TeamT::kMarch) mop_matvec(A, D, *tm.mt, tm.cta(), tm.ncta(), pq);
+    if constexpr (TeamT::kFlat) fop_matvec(A, D, *tm.fs, tm.cta(), tm.ncta(), pq);
     else op_matvec(A, D, (int)tm.t(), (int)tm.T(), pq);
 }
 template <class R, class TeamT>
 __device__ __forceinline__ void t_update(const KArena& A, const KDesc& D, TeamT& tm, float alpha, R& rr) {
-    if constexpr (TeamT::kMarch) vop_update(A, D, (int)tm.t(), (int)tm.T(), alpha, rr);
+    if constexpr (TeamT::kFlat) vop_update(A, D, (int)tm.t(), (int)tm.T(), alpha, rr);
     else op_update(A, D, (int)tm.t(), (int)tm.T(), alpha, rr);
 }
 template <class R, class TeamT>
 __device__ __forceinline__ void t_dot_rz(const KArena& A, const KDesc& D, TeamT& tm, R& rz) {
-    if constexpr (TeamT::kMarch) vop_dot_rz(A, D, (int)tm.t(), (int)tm.T(), rz);
+    if constexpr (TeamT::kFlat) vop_dot_rz(A, D, (int)tm.t(), (int)tm.T(), rz);
     else op_dot_rz(A, D, (int)tm.t(), (int)tm.T(), rz);
 }
 template <class TeamT>
 __device__ __forceinline__ void t_pupdate(const KArena& A, const KDesc& D, TeamT& tm, float beta) {
-    if constexpr (TeamT::kMarch) vop_pupdate(A, D, (int)tm.t(), (int)tm.T(), beta);
+    if constexpr (TeamT::kFlat) vop_pupdate(A, D, (int)tm.t(), (int)tm.T(), beta);
     else op_pupdate(A, D, (int)tm.t(), (int)tm.T(), beta);
 }
 template <class TeamT>
 __device__ __forceinline__ void t_accumulate(const KArena& A, const KDesc& D, TeamT& tm) {
-    if constexpr (TeamT::kMarch) vop_accumulate(A, D, (int)tm.t(), (int)tm.T());
+    if constexpr (TeamT::kFlat) vop_accumulate(A, D, (int)tm.t(), (int)tm.T());
     else op_accumulate(A, D, (int)tm.t(), (int)tm.T());
 }
 template <int P, class TeamT>
 __device__ __forceinline__ void t_restrict0(const KArena& A, const KDesc& D, TeamT& tm) {
-    if constexpr (TeamT::kMarch) mop_restrict0<P>(A, D, *tm.mt, tm.cta(), tm.ncta());
+    if constexpr (TeamT::kFlat) fop_restrict0<P>(A, D, *tm.fs, tm.cta(), tm.ncta());
     else op_restrict0<P>(A, D, (int)tm.t(), (int)tm.T());
 }
 template <class TeamT>
 __device__ __forceinline__ void t_cheb0_first(const KArena& A, const KDesc& D, TeamT& tm, float c2, float* zout) {
-    if constexpr (TeamT::kMarch) vop_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2, zout);
+    if constexpr (TeamT::kFlat) vop_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2, zout);
     else op_cheb0_first(A, D, (int)tm.t(), (int)tm.T(), c2, zout);
 }
 template <int P, class TeamT>
 __device__ __forceinline__ void t_cheb0_dz(const KArena& A, const KDesc& D, TeamT& tm, const float* zin, float* zout,
                                            float c1, float c2) {
-    if constexpr (TeamT::kMarch) mop_cheb0_dz<P>(A, D, *tm.mt, tm.cta(), tm.ncta(), zin, zout, c1, c2);
+    if constexpr (TeamT::kFlat) fop_cheb0_dz<P>(A, D, *tm.fs, tm.cta(), tm.ncta(), zin, zout, c1, c2);
     else op_cheb0_dz<P>(A, D, (int)tm.t(), (int)tm.T(), zin, zout, c1, c2);
 }
 template <class TeamT>
 __device__ __forceinline__ void t_copy(const KDesc& D, TeamT& tm, const float* src, float* dst) {
-    if constexpr (TeamT::kMarch) vop_copy((int)tm.t(), (int)tm.T(), (int)D.n, src, dst);
+    if constexpr (TeamT::kFlat) vop_copy((int)tm.t(), (int)tm.T(), (int)D.n, src, dst);
     else op_copy((int)tm.t(), (int)tm.T(), (int)D.n, src, dst);
 }
 
@@ -454,6 +461,11 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         op_dinv0<P>(A, D, t, T);
         tm.sync();
     }
+    if constexpr (TeamT::kFlat) {
+        // the marching passes never write non-solid voxels: q starts at zero
+        vop_zero(t, T, (int)D.n, A.q + D.off);
+        flat_lists(A, D, *tm.fs, tm);
+    }
     const unsigned long long t_built = globaltimer();
     unsigned long long t_pc = 0;  // time in V-cycles (the leader's clock, between barriers)
     VTimes vt;
@@ -530,9 +542,10 @@ template <int P>
 __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
     k_grid(const __grid_constant__ KArena A, int ngiant) {
     __shared__ SharedScratch sh;
-    __shared__ MarchTile mt;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    FlatSmem& fs = *reinterpret_cast<FlatSmem*>(dyn_smem);
     GridTeam tm{&sh, reinterpret_cast<unsigned*>(A.queue + 8), reinterpret_cast<unsigned*>(A.queue + 9), A.queue + 10,
-                reinterpret_cast<double*>(A.scratch), &mt};
+                reinterpret_cast<double*>(A.scratch), &fs};
     for (int q = 0; q < ngiant; q++) {
         KDesc& D = A.desc[A.order[q]];
         if (A.fp64_dots) team_solve<P, double>(A, D, tm);
@@ -548,9 +561,11 @@ template <int P, int C>
 __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
     k_batched(const __grid_constant__ KArena A, int base, int nbig, int nsmall) {
     __shared__ SharedScratch sh;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    FlatSmem& fs = *reinterpret_cast<FlatSmem*>(dyn_smem);
     if constexpr (C > 1) {
         cg::cluster_group cl = cg::this_cluster();
-        ClusterTeam<C> tm{&sh};
+        ClusterTeam<C> tm{&sh, &fs};
         for (;;) {
             if (cl.block_rank() == 0 && threadIdx.x == 0) sh.next = atomicAdd(&A.queue[0], 1);
             cl.sync();
@@ -563,7 +578,7 @@ __global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
         }
         cl.sync();  // no CTA leaves while a peer may still read its shared memory
     }
-    CtaTeam tm{&sh};
+    CtaTeam tm{&sh, &fs};
     const int nmid_end = A.nisl - nsmall;
     for (;;) {
         if (threadIdx.x == 0) sh.next = atomicAdd(&A.queue[1], 1);
@@ -596,7 +611,9 @@ template <int P>
 cudaError_t launch_grid(cudaStream_t s, const KArena& a, int ngiant, int num_sms) {
     auto kern = k_grid<P>;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, 0) != cudaSuccess ||
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FlatSmem)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, sizeof(FlatSmem)) !=
+            cudaSuccess ||
         per_sm <= 0)
         return cudaErrorInvalidConfiguration;
     const int ctas = std::min(num_sms * per_sm, kGridMaxBlocks);
@@ -606,7 +623,7 @@ cudaError_t launch_grid(cudaStream_t s, const KArena& a, int ngiant, int num_sms
     attr[0].val.cooperative = 1;
     cfg.gridDim = dim3(ctas);
     cfg.blockDim = dim3(kBatchedThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = sizeof(FlatSmem);
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
@@ -619,10 +636,14 @@ cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int 
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
     cfg.blockDim = dim3(kBatchedThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = sizeof(FlatSmem);
     cfg.stream = s;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FlatSmem)) !=
+        cudaSuccess)
+        return cudaErrorInvalidConfiguration;
     int per_sm = kBatchedMinBlocks;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, sizeof(FlatSmem)) !=
+            cudaSuccess ||
         per_sm <= 0) {
         cudaGetLastError();
         per_sm = 1;

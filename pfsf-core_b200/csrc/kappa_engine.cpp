@@ -109,7 +109,7 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     free_arena();
     auto A = std::make_unique<Arena>();
     A->prec = (int)precision_;
-    int64_t fine = 0, coarse = 0;
+    int64_t fine = 0, coarse = 0, starts = 0;
     for (Island* s : set) {
         KDesc d{};
         d.lx = s->lx; d.ly = s->ly; d.lz = s->lz;
@@ -121,6 +121,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
             d.lev[l].off = coarse;
             coarse = align_up(coarse + d.lev[l].n, kAlignElems);
         }
+        d.soff = starts;
+        starts = align_up(starts + flat_starts(s->lx, s->ly, s->lz), kAlignElems);
         A->desc.push_back(d);
         A->ids.push_back(s->id);
         const uint8_t* t = static_cast<const uint8_t*>(s->hosts.k_type);
@@ -141,7 +143,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
                  o_cx = take(coarse * 4), o_cb = take(coarse * 4), o_desc = take(sizeof(KDesc) * nisl),
                  o_order = take(sizeof(int) * nisl), o_queue = take(256),
                  o_scr = take(sizeof(float) * kappa::plain_scratch_floats()), o_dinv = take(fine * 4),
-                 o_d0 = take(fine * 4), o_cdd = take(coarse * 4), o_cx2 = take(coarse * 4);
+                 o_d0 = take(fine * 4), o_cdd = take(coarse * 4), o_cx2 = take(coarse * 4),
+                 o_flist = take(fine * 4), o_fstart = take((size_t)std::max<int64_t>(starts, 1) * 4);
     A->bytes = off;
     if (fault_alloc_after_ >= 0 && alloc_count_ >= fault_alloc_after_) return false;
     if (cudaMalloc(&A->base, A->bytes) != cudaSuccess) {
@@ -179,6 +182,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     k.d0 = reinterpret_cast<float*>(b + o_d0);
     k.cd = reinterpret_cast<float*>(b + o_cdd);
     k.cx2 = reinterpret_cast<float*>(b + o_cx2);
+    k.flist = reinterpret_cast<uint32_t*>(b + o_flist);
+    k.fstart = reinterpret_cast<int*>(b + o_fstart);
     k.nisl = nisl;
     k.prec = A->prec;
     if (!CU_OK(cudaMallocHost((void**)&A->hscratch, 256))) return false;

@@ -1,0 +1,519 @@
+// Fine-level passes of CTA-granular teams (one CTA, a thread-block cluster,
+// the whole GPU): plane-tile marching over per-plane solid-voxel lists, and
+// four-wide streaming ops.
+//
+// The generic ops in kappa_ops.cuh give every thread a strided list of
+// voxels and gather each voxel's 26 neighbours from global memory; within
+// 64 registers per thread they keep only one plane's loads in flight, so the
+// passes are latency bound, and the lanes of air voxels idle through the
+// stencil arithmetic of their solid neighbours in the warp.  Here a CTA takes
+// a work item of tx x ty columns (kFlatCap cells per plane with the one-voxel
+// halo, see flat_tile) by a run of planes and marches up the planes with a
+// 4-plane ring of the input vector and of 1/kappa in shared memory: plane
+// z+2 is fetched into registers while plane z is computed, then stored into
+// the slot plane z-2 used.  Plane z is computed only at its solid voxels,
+// taken from a list per (tile, plane) built once per solve (flat_lists), so
+// every active lane does stencil work.
+//
+// Link weight.  The harmonic mean is evaluated as kappa_i kappa_j /
+// (kappa_i + kappa_j) = 1 / (1/kappa_i + 1/kappa_j), with the reciprocals
+// staged once per cell (rcp.approx: 1/0 = +inf, so an air or out-of-box
+// neighbour gets weight 1/(r_i + inf) = 0 with no test), and the 26 terms
+// are summed per link class (faces x2, edges x1, corners x1/3).  Results
+// equal the generic ops' up to FP32 rounding; both are the same operator.
+//
+// Invariant relied on: the vectors marched here (z, q, p) are zero on every
+// non-solid voxel.  The outer residual zeroes z, p = z + beta p keeps p's
+// zeros, and the solve clears q once at its start (team_solve), so the
+// passes never write non-solid voxels.
+#pragma once
+#include "kappa_ops.cuh"
+
+namespace pfsf_b200 {
+namespace kappa {
+namespace {
+
+struct FlatSmem {
+    float v[4][kFlatCap];  // vector ring
+    float w[4][kFlatCap];  // 1/kappa ring
+};
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ int fslot(int z) { return (z + 4) & 3; }
+
+struct FlatGeom {
+    int tx, ty, hx, hp, ntx, ntiles, zc, nwork;
+};
+// Tiles of the island, and work items of zc planes: the whole depth for a
+// single-CTA team; when ncta CTAs share the island, runs of planes long
+// enough that every CTA gets at most one work item if the tiles allow it
+// (each work item re-reads 3 planes, so runs stay at least kFlatZ / 2 long),
+// else kFlatZ.  zc is even, so plane pairs of one aggregate stay together.
+__device__ __forceinline__ FlatGeom flat_geom(const KDesc& D, int ncta) {
+    FlatGeom G;
+    flat_tile(D.lx, D.ly, G.tx, G.ty);
+    G.hx = G.tx + 2;
+    G.hp = G.hx * (G.ty + 2);
+    G.ntx = (D.lx + G.tx - 1) / G.tx;
+    G.ntiles = G.ntx * ((D.ly + G.ty - 1) / G.ty);
+    if (ncta == 1) {
+        G.zc = D.lz;
+    } else {
+        const int nz = ncta / G.ntiles;
+        G.zc = nz >= 1 ? max(kFlatZ / 2, (((D.lz + nz - 1) / nz) + 1) & ~1) : kFlatZ;
+    }
+    G.nwork = G.ntiles * ((D.lz + G.zc - 1) / G.zc);
+    return G;
+}
+
+struct FlatPlanes {
+    const float *vm, *v0, *vp, *wm, *w0, *wp;
+    float* spare;  // the vector slot of plane z-2: free until the step ends
+};
+
+// 26-neighbour sum of w_ij (z_i - z_j) at halo cell hc
+__device__ __forceinline__ float flat_az(const FlatPlanes& P, int hc, int hx, float zi, float ri) {
+    float af = 0.0f, ae = 0.0f, ac = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+        for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+            for (int dx = -1; dx <= 1; dx++) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                const int o = hc + dy * hx + dx;
+                const float zj = (dz < 0 ? P.vm : (dz > 0 ? P.vp : P.v0))[o];
+                const float rj = (dz < 0 ? P.wm : (dz > 0 ? P.wp : P.w0))[o];
+                const float t = rcp_approx(ri + rj) * (zi - zj);
+                const int g = (dx != 0) + (dy != 0) + (dz != 0);
+                if (g == 1) af += t;
+                else if (g == 2) ae += t;
+                else ac += t;
+            }
+    return 2.0f * af + ae + (1.0f / 3.0f) * ac;
+}
+
+// This thread's entries of one (tile, plane) solid list (bounds b0, b1):
+// at most kFlatCap / kFlatThreads, ~0u past the end.
+__device__ __forceinline__ void flat_entries(const uint32_t* L, int b0, int b1,
+                                             uint32_t (&e)[kFlatCap / kFlatThreads]) {
+#pragma unroll
+    for (int k = 0; k < kFlatCap / kFlatThreads; k++) {
+        const int j = b0 + (int)threadIdx.x + kFlatThreads * k;
+        e[k] = j < b1 ? L[j] : ~0u;
+    }
+}
+
+// March over every work item this CTA owns (cta, cta + ncta, ...).
+// body(tile, x0, y0, z, z0, z1, planes, entries) runs on every thread once
+// per plane (it may hold CTA barriers); vload / kload read the vector and
+// kappa of island voxel g.  With kList the march also pipelines the solid
+// lists (L, st): entries of plane z+1 and the list bounds of plane z+2 load
+// while plane z is computed, so a step waits on one round of global loads
+// (the per-voxel operands), not three.
+template <bool kList, class VLoad, class KLoad, class Body>
+__device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int cta, int ncta, const uint32_t* L,
+                           const int* st, VLoad vload, KLoad kload, Body body) {
+    constexpr int J = kFlatCap / kFlatThreads;
+    const int tid = threadIdx.x;
+    for (int w = cta; w < G.nwork; w += ncta) {
+        const int tile = w % G.ntiles, zk = w / G.ntiles;
+        const int x0 = (tile % G.ntx) * G.tx, y0 = (tile / G.ntx) * G.ty;
+        const int z0 = zk * G.zc, z1 = min(z0 + G.zc, D.lz);
+        auto fetch = [&](int z, int e, float& v, float& k) {
+            v = 0.0f;
+            k = 0.0f;
+            if (e >= G.hp || z < 0 || z >= D.lz) return;
+            const int hy = e / G.hx, hx = e - hy * G.hx;
+            const int x = x0 - 1 + hx, y = y0 - 1 + hy;
+            if (x < 0 || x >= D.lx || y < 0 || y >= D.ly) return;
+            const int g = x + D.lx * (y + D.ly * z);
+            v = vload(g);
+            k = kload(g);
+        };
+        uint32_t cur[J], nxt[J];
+        int nb0 = 0, nb1 = 0;  // list bounds of plane z+1 (then z+2)
+        if constexpr (kList) {
+            const int p = tile * D.lz + z0;
+            flat_entries(L, st[p], st[p + 1], cur);
+            if (z0 + 1 < z1) {
+                nb0 = st[p + 1];
+                nb1 = st[p + 2];
+            }
+        }
+        for (int pz = z0 - 1; pz <= z0 + 1; pz++) {
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const int e = tid + kFlatThreads * j;
+                float v, k;
+                fetch(pz, e, v, k);
+                if (e < G.hp) {
+                    S.v[fslot(pz)][e] = v;
+                    S.w[fslot(pz)][e] = rcp_approx(k);
+                }
+            }
+        }
+        __syncthreads();
+        for (int z = z0; z < z1; z++) {
+            float pv[J], pk[J];
+#pragma unroll
+            for (int j = 0; j < J; j++) fetch(z + 2, tid + kFlatThreads * j, pv[j], pk[j]);
+            if constexpr (kList) {
+                flat_entries(L, nb0, nb1, nxt);
+                const int p2 = tile * D.lz + z + 2;
+                nb0 = z + 2 < z1 ? st[p2] : 0;
+                nb1 = z + 2 < z1 ? st[p2 + 1] : 0;
+            }
+            const FlatPlanes P{S.v[fslot(z - 1)], S.v[fslot(z)], S.v[fslot(z + 1)],
+                               S.w[fslot(z - 1)], S.w[fslot(z)], S.w[fslot(z + 1)], S.v[fslot(z + 2)]};
+            body(tile, x0, y0, z, z0, z1, P, cur);
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const int e = tid + kFlatThreads * j;
+                if (e < G.hp) {
+                    S.v[fslot(z + 2)][e] = pv[j];
+                    S.w[fslot(z + 2)][e] = rcp_approx(pk[j]);
+                }
+            }
+            if constexpr (kList) {
+#pragma unroll
+                for (int j = 0; j < J; j++) cur[j] = nxt[j];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---- the per-(tile, plane) solid lists
+
+// Builds the island's lists: counts per (tile, plane), an inclusive scan by
+// the team's first CTA, then each (tile, plane) writes its solid columns in
+// column order (deterministic).  Ends with a team barrier.
+template <class TeamT>
+__device__ void flat_lists(const KArena& A, const KDesc& D, FlatSmem& S, TeamT& tm) {
+    const FlatGeom G = flat_geom(D, 1);
+    const int m = G.ntiles * D.lz, cells = G.tx * G.ty;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint8_t* type = A.type + D.off;
+    int* st = A.fstart + D.soff;
+    uint32_t* L = A.flist + D.off;
+    int* sm = reinterpret_cast<int*>(S.v[0]);  // no march in progress
+    auto solid_at = [&](int p, int c, uint32_t& pc) {
+        const int tile = p / D.lz, z = p - tile * D.lz;
+        const int cy = c / G.tx, cx = c - cy * G.tx;
+        const int x = (tile % G.ntx) * G.tx + cx, y = (tile / G.ntx) * G.ty + cy;
+        pc = (uint32_t)cx | ((uint32_t)cy << 16);
+        return c < cells && x < D.lx && y < D.ly && type[x + D.lx * (y + D.ly * z)] == kSolid;
+    };
+    for (int p = tm.cta(); p < m; p += tm.ncta()) {
+        int cnt = 0;
+        for (int c0 = 0; c0 < cells; c0 += kFlatThreads) {
+            uint32_t pc;
+            cnt += __syncthreads_count(solid_at(p, c0 + tid, pc));
+        }
+        if (tid == 0) st[p + 1] = cnt;
+    }
+    tm.sync();
+    if (tm.cta() == 0) {
+        int carry = 0;
+        for (int c0 = 0; c0 < m; c0 += kFlatThreads) {
+            const int k = c0 + tid;
+            int v = k < m ? st[k + 1] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += u;
+            }
+            if (lane == 31) sm[wid] = v;
+            __syncthreads();
+            if (wid == 0) {
+                int s = lane < kFlatThreads / 32 ? sm[lane] : 0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, s, o);
+                    if (lane >= o) s += u;
+                }
+                if (lane < kFlatThreads / 32) sm[32 + lane] = s;
+            }
+            __syncthreads();
+            v += carry + (wid > 0 ? sm[32 + wid - 1] : 0);
+            if (k < m) st[k + 1] = v;
+            carry += sm[32 + kFlatThreads / 32 - 1];
+            __syncthreads();
+        }
+        if (tid == 0) st[0] = 0;
+    }
+    tm.sync();
+    for (int p = tm.cta(); p < m; p += tm.ncta()) {
+        int base = st[p];
+        for (int c0 = 0; c0 < cells; c0 += kFlatThreads) {
+            uint32_t pc;
+            const bool s = solid_at(p, c0 + tid, pc);
+            const unsigned ball = __ballot_sync(0xffffffffu, s);
+            if (lane == 0) sm[wid] = __popc(ball);
+            __syncthreads();
+            int off = base + __popc(ball & ((1u << lane) - 1u));
+            int total = 0;
+            for (int k = 0; k < kFlatThreads / 32; k++) {
+                const int c = sm[k];
+                off += k < wid ? c : 0;
+                total += c;
+            }
+            if (s) L[off] = pc;
+            base += total;
+            __syncthreads();
+        }
+    }
+    tm.sync();
+}
+
+// ---- the marching forms of the fine-level stencil ops
+
+// one whole Chebyshev step out of place (op_cheb0_dz), solid voxels only
+template <int P>
+__device__ void fop_cheb0_dz(const KArena& A, const KDesc& D, FlatSmem& S, int cta, int ncta, const float* zin,
+                             float* zout, float c1, float c2) {
+    const Fine F = fine_view(A, D);
+    const float* dinv = A.dinv0 + D.off;
+    float* d = A.d0 + D.off;
+    const uint32_t* L = A.flist + D.off;
+    const int* st = A.fstart + D.soff;
+    const FlatGeom G = flat_geom(D, ncta);
+    flat_march<true>(D, G, S, cta, ncta, L, st, [&](int g) { return zin[g]; }, [&](int g) { return kpre<P>(F, g); },
+                     [&](int, int x0, int y0, int z, int, int, const FlatPlanes& Pl, const uint32_t(&ent)[kFlatCap / kFlatThreads]) {
+#pragma unroll
+                         for (int k = 0; k < kFlatCap / kFlatThreads; k++) {
+                             const uint32_t pc = ent[k];
+                             if (pc == ~0u) break;
+                             const int cx = (int)(pc & 0xffffu), cy = (int)(pc >> 16);
+                             const int i = x0 + cx + F.lx * (y0 + cy + F.ly * z);
+                             const int hc = (cy + 1) * G.hx + cx + 1;
+                             const float zi = Pl.v0[hc];
+                             const float az = flat_az(Pl, hc, G.hx, zi, Pl.w0[hc]);
+                             const float upd = c2 * dinv[i] * (F.r[i] - az);
+                             const float dn = c1 == 0.0f ? upd : c1 * d[i] + upd;
+                             d[i] = dn;
+                             zout[i] = zi + dn;
+                         }
+                     });
+}
+
+// q = A p (FP32 kappa) at solid voxels; returns this thread's share of p.q
+template <class R>
+__device__ void fop_matvec(const KArena& A, const KDesc& D, FlatSmem& S, int cta, int ncta, R& pq) {
+    const Fine F = fine_view(A, D);
+    const uint32_t* L = A.flist + D.off;
+    const int* st = A.fstart + D.soff;
+    const FlatGeom G = flat_geom(D, ncta);
+    flat_march<true>(D, G, S, cta, ncta, L, st, [&](int g) { return F.p[g]; }, [&](int g) { return F.k32[g]; },
+                     [&](int, int x0, int y0, int z, int, int, const FlatPlanes& Pl, const uint32_t(&ent)[kFlatCap / kFlatThreads]) {
+#pragma unroll
+                         for (int k = 0; k < kFlatCap / kFlatThreads; k++) {
+                             const uint32_t pc = ent[k];
+                             if (pc == ~0u) break;
+                             const int cx = (int)(pc & 0xffffu), cy = (int)(pc >> 16);
+                             const int i = x0 + cx + F.lx * (y0 + cy + F.ly * z);
+                             const int hc = (cy + 1) * G.hx + cx + 1;
+                             const float pi = Pl.v0[hc];
+                             const float acc = flat_az(Pl, hc, G.hx, pi, Pl.w0[hc]);
+                             F.q[i] = acc;
+                             pq += (R)pi * (R)acc;
+                         }
+                     });
+}
+
+// Residual of level 0 (operator A') summed over each 2x2x2 aggregate into
+// level 1, x1 = 0.  Every column of the tile, solid or not, keeps one thread
+// for the whole march: plane pairs add in registers, then the 2 x 2 column
+// groups through the ring's spare slot.  Tiles and work items start on even x, y, z,
+// so every aggregate lies in one work item.  (Summation order differs from
+// op_restrict0's child order: equal up to FP32 rounding.)
+template <int P>
+__device__ void fop_restrict0(const KArena& A, const KDesc& D, FlatSmem& S, int cta, int ncta) {
+    constexpr int J = kFlatCap / kFlatThreads;
+    const Fine F = fine_view(A, D);
+    const Coarse C = coarse_view(A, D, 1);
+    const FlatGeom G = flat_geom(D, ncta);
+    const int tid = threadIdx.x, cells = G.tx * G.ty;
+    const int ctx = (G.tx + 1) >> 1, cty = (G.ty + 1) >> 1;
+    int cxj[J], cyj[J];
+#pragma unroll
+    for (int j = 0; j < J; j++) {
+        const int c = tid + kFlatThreads * j;
+        cyj[j] = c / G.tx;
+        cxj[j] = c - cyj[j] * G.tx;
+    }
+    float hold[J];
+    flat_march<false>(D, G, S, cta, ncta, nullptr, nullptr, [&](int g) { return F.z[g]; },
+                      [&](int g) { return kpre<P>(F, g); },
+                      [&](int, int x0, int y0, int z, int z0, int z1, const FlatPlanes& Pl,
+                          const uint32_t(&)[kFlatCap / kFlatThreads]) {
+                   const bool second = ((z - z0) & 1) != 0;
+#pragma unroll
+                   for (int j = 0; j < J; j++) {
+                       const int c = tid + kFlatThreads * j;
+                       const int x = x0 + cxj[j], y = y0 + cyj[j];
+                       float res = 0.0f;
+                       if (c < cells && x < F.lx && y < F.ly) {
+                           const int i = x + F.lx * (y + F.ly * z);
+                           if (F.type[i] == kSolid) {
+                               const int hc = (cyj[j] + 1) * G.hx + cxj[j] + 1;
+                               const float zi = Pl.v0[hc];
+                               res = F.r[i] - flat_az(Pl, hc, G.hx, zi, Pl.w0[hc]);
+                           }
+                       }
+                       hold[j] = second ? hold[j] + res : res;
+                   }
+                   if (!second && z != z1 - 1) return;
+#pragma unroll
+                   for (int j = 0; j < J; j++) {
+                       const int c = tid + kFlatThreads * j;
+                       if (c < cells) Pl.spare[c] = hold[j];
+                   }
+                   __syncthreads();
+                   const int gz = z >> 1;
+                   for (int cc = tid; cc < ctx * cty; cc += kFlatThreads) {
+                       const int ccy = cc / ctx, ccx = cc - ccy * ctx;
+                       float s = 0.0f;
+#pragma unroll
+                       for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                           for (int dx = 0; dx < 2; dx++) {
+                               const int ux = 2 * ccx + dx, uy = 2 * ccy + dy;
+                               if (ux < G.tx && uy < G.ty) s += Pl.spare[uy * G.tx + ux];
+                           }
+                       const int gx = (x0 >> 1) + ccx, gy = (y0 >> 1) + ccy;
+                       if (gx < C.lx && gy < C.ly && gz < C.lz) {
+                           const int c = gx + C.lx * (gy + C.ly * gz);
+                           C.b[c] = s;
+                           C.x[c] = 0.0f;
+                       }
+                   }
+                   __syncthreads();  // the march stores plane z+2 into the spare slot next
+               });
+}
+
+// ---- streaming ops, four voxels per access (island arrays start 128-byte aligned)
+template <class R>
+__device__ void vop_update(const KArena& A, const KDesc& D, int t, int T, float alpha, R& rr) {
+    const Fine F = fine_view(A, D);
+    const int n4 = F.n >> 2;
+    float4* r4 = reinterpret_cast<float4*>(F.r);
+    float4* e4 = reinterpret_cast<float4*>(F.e);
+    const float4* q4 = reinterpret_cast<const float4*>(F.q);
+    const float4* p4 = reinterpret_cast<const float4*>(F.p);
+    for (int j = t; j < n4; j += T) {
+        float4 r = r4[j], e = e4[j];
+        const float4 q = q4[j], p = p4[j];
+        r.x -= alpha * q.x; r.y -= alpha * q.y; r.z -= alpha * q.z; r.w -= alpha * q.w;
+        e.x += alpha * p.x; e.y += alpha * p.y; e.z += alpha * p.z; e.w += alpha * p.w;
+        r4[j] = r;
+        e4[j] = e;
+        rr += (R)r.x * (R)r.x + (R)r.y * (R)r.y + (R)r.z * (R)r.z + (R)r.w * (R)r.w;
+    }
+    for (int i = 4 * n4 + t; i < F.n; i += T) {
+        const float ri = F.r[i] - alpha * F.q[i];
+        F.e[i] += alpha * F.p[i];
+        F.r[i] = ri;
+        rr += (R)ri * (R)ri;
+    }
+}
+
+template <class R>
+__device__ void vop_dot_rz(const KArena& A, const KDesc& D, int t, int T, R& rz) {
+    const Fine F = fine_view(A, D);
+    const int n4 = F.n >> 2;
+    const float4* r4 = reinterpret_cast<const float4*>(F.r);
+    const float4* z4 = reinterpret_cast<const float4*>(F.z);
+    for (int j = t; j < n4; j += T) {
+        const float4 r = r4[j], z = z4[j];
+        rz += (R)r.x * (R)z.x + (R)r.y * (R)z.y + (R)r.z * (R)z.z + (R)r.w * (R)z.w;
+    }
+    for (int i = 4 * n4 + t; i < F.n; i += T) rz += (R)F.r[i] * (R)F.z[i];
+}
+
+__device__ void vop_pupdate(const KArena& A, const KDesc& D, int t, int T, float beta) {
+    const Fine F = fine_view(A, D);
+    const int n4 = F.n >> 2;
+    float4* p4 = reinterpret_cast<float4*>(F.p);
+    float4* z4 = reinterpret_cast<float4*>(F.z);
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int j = t; j < n4; j += T) {
+        const float4 z = z4[j];
+        float4 p;
+        if (beta == 0.0f) {
+            p = z;
+        } else {
+            p = p4[j];
+            p.x = z.x + beta * p.x; p.y = z.y + beta * p.y; p.z = z.z + beta * p.z; p.w = z.w + beta * p.w;
+        }
+        p4[j] = p;
+        z4[j] = zero;
+    }
+    for (int i = 4 * n4 + t; i < F.n; i += T) {
+        const float zi = F.z[i];
+        F.p[i] = beta == 0.0f ? zi : zi + beta * F.p[i];
+        F.z[i] = 0.0f;
+    }
+}
+
+// zout: F.z or the q array (both island arrays, 128-byte aligned)
+__device__ void vop_cheb0_first(const KArena& A, const KDesc& D, int t, int T, float c2, float* zout) {
+    const Fine F = fine_view(A, D);
+    const int n4 = F.n >> 2;
+    const float4* dv4 = reinterpret_cast<const float4*>(A.dinv0 + D.off);
+    const float4* r4 = reinterpret_cast<const float4*>(F.r);
+    float4* d4 = reinterpret_cast<float4*>(A.d0 + D.off);
+    float4* z4 = reinterpret_cast<float4*>(zout);
+    for (int j = t; j < n4; j += T) {
+        const float4 dv = dv4[j], r = r4[j];
+        const float4 v = make_float4(c2 * dv.x * r.x, c2 * dv.y * r.y, c2 * dv.z * r.z, c2 * dv.w * r.w);
+        d4[j] = v;
+        z4[j] = v;
+    }
+    const float* dinv = A.dinv0 + D.off;
+    float* d = A.d0 + D.off;
+    for (int i = 4 * n4 + t; i < F.n; i += T) {
+        const float v = c2 * dinv[i] * F.r[i];
+        d[i] = v;
+        zout[i] = v;
+    }
+}
+
+__device__ void vop_zero(int t, int T, int n, float* dst) {
+    const int n4 = n >> 2;
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int j = t; j < n4; j += T) d4[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int i = 4 * n4 + t; i < n; i += T) dst[i] = 0.0f;
+}
+
+__device__ void vop_copy(int t, int T, int n, const float* src, float* dst) {
+    const int n4 = n >> 2;
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int j = t; j < n4; j += T) d4[j] = s4[j];
+    for (int i = 4 * n4 + t; i < n; i += T) dst[i] = src[i];
+}
+
+__device__ void vop_accumulate(const KArena& A, const KDesc& D, int t, int T) {
+    const Fine F = fine_view(A, D);
+    const int n4 = F.n >> 2;
+    const float4* e4 = reinterpret_cast<const float4*>(F.e);
+    double2* x2 = reinterpret_cast<double2*>(F.x64);
+    for (int j = t; j < n4; j += T) {
+        const float4 e = e4[j];
+        double2 a = x2[2 * j], b = x2[2 * j + 1];
+        a.x += (double)e.x; a.y += (double)e.y; b.x += (double)e.z; b.y += (double)e.w;
+        x2[2 * j] = a;
+        x2[2 * j + 1] = b;
+    }
+    for (int i = 4 * n4 + t; i < F.n; i += T) F.x64[i] += (double)F.e[i];
+}
+
+}  // namespace
+}  // namespace kappa
+}  // namespace pfsf_b200

@@ -7,6 +7,8 @@ solve (tol 1e-12) to <= 1e-4 relative (inf-norm), which is what a 1e-6
 residual allows for condition numbers ~L^2.  The FP32 phi written back is
 that accumulator rounded.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -92,6 +94,44 @@ def test_batched_uneven_islands(eng):
     assert inner == st.inner_iterations_total
     rc, _ = eng.island_report(987654)
     assert rc == capi.PFSF_ERROR_INVALID_ARG
+
+
+@pytest.mark.parametrize("cluster", ["8", "16", "1"])
+def test_tile_shapes_and_teams(lib_built, cluster):
+    """Every team that marches plane tiles (one CTA, 8- and 16-CTA clusters,
+    the whole GPU) on islands whose sides need several tiles: x wider than
+    one 126-column tile, y split into bands, odd depths and odd widths (an
+    aggregate of the next level cut by the island edge)."""
+    env = {"PFSF_CLUSTER_MIN_VOXELS": "20000", "PFSF_GRID_MIN_VOXELS": "60000", "PFSF_CLUSTER": cluster}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        e = capi.Engine(capi.default_config(max_island_size=1 << 26, tick_budget_ms=1 << 30))
+        assert e.init() == capi.PFSF_OK
+    finally:
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
+    try:
+        e.set_solve_mode(capi.SOLVE_BATCHED)
+        e.set_precision(capi.PREC_BF16)
+        dims = [(131, 9, 5), (127, 40, 7), (7, 300, 6), (33, 31, 17), (141, 23, 21), (9, 11, 13), (250, 30, 9)]
+        isls = [synth.noise_island(d, seed=40 + k) for k, d in enumerate(dims)]
+        isls = [i for i in isls if i.n_active > 0]
+        reg = [_register(e, isl) for isl in isls]
+        rc, st = e.solve([r[0] for r in reg], tol=TOL)
+        assert rc == capi.PFSF_OK
+        assert st.islands_converged == len(isls), st.max_rel_residual
+        teams = set()
+        for isl, (iid, host) in zip(isls, reg):
+            _check(e, isl, iid, host)
+            rc, r = e.island_report(iid)
+            teams.add(capi.IslandReport.TEAMS[r.team])
+        assert "grid" in teams and "cta" in teams and ("cluster" in teams or cluster == "1")
+    finally:
+        e.close()
 
 
 def test_warm_start_resolve_is_immediate(eng):
