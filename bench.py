@@ -406,8 +406,9 @@ def run_ours(args):
                          "vcycle_ms_sum": {"fine": stats[-1].vcycle_fine_ms_sum,
                                            "coarse": stats[-1].vcycle_coarse_ms_sum,
                                            "tail": stats[-1].vcycle_tail_ms_sum},
-                         "cluster": os.environ.get("PFSF_CLUSTER", "8"),
-                         "cluster_min_voxels": os.environ.get("PFSF_CLUSTER_MIN_VOXELS", "131072"),
+                         "persistent_ctas": stats[-1].persistent_ctas,
+                         "cluster": os.environ.get("PFSF_CLUSTER", "4"),
+                         "cluster_min_voxels": os.environ.get("PFSF_CLUSTER_MIN_VOXELS", "262144"),
                          "warp_max_voxels": os.environ.get("PFSF_WARP_MAX_VOXELS", "0"),
                          "smoother": os.environ.get("PFSF_SMOOTHER", "chebyshev(batched)"), "cheb_k": os.environ.get("PFSF_CHEB_K", "3")},
         }

@@ -69,6 +69,8 @@ typedef struct pfsf_solve_stats {
     double vcycle_fine_ms_sum;      /* ... of which fine-level passes */
     double vcycle_coarse_ms_sum;    /* ... coarse levels smoothed by the whole team */
     double vcycle_tail_ms_sum;      /* ... the coarsest levels (single warp or team) */
+    int32_t persistent_ctas;        /* batched mode: CTAs of the persistent launch(es) */
+    int32_t reserved;
 } pfsf_solve_stats;
 
 /* Registers the kappa-form inputs of an island created by pfsf_add_island.

@@ -20,6 +20,7 @@ struct Engine::Arena {
     float* phi_out = nullptr;        // FP32 solution staging (device), aliases e
     std::vector<void*> pinned;       // host ranges registered for fast copies
     bool solved = false;             // x64 holds a forward solution of this island set
+    int persistent_ctas = 0;         // CTAs of the last batched launch(es)
     bool b_stale = false;            // b holds an adjoint right-hand side, not the sources
     double* xf = nullptr;            // adjoint: FP64 copy of the forward solution (own allocation)
 };

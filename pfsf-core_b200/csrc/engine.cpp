@@ -64,6 +64,14 @@ pfsf_result Engine::init() {
     device_ = dev;
     cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev);
     if (!CU_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) return PFSF_ERROR_VULKAN;
+    // side stream of the batched solve (fills CTA slots clusters leave free);
+    // without it the solve runs on stream_ alone
+    if (!CU_OK(cudaStreamCreateWithFlags(&side_.stream, cudaStreamNonBlocking)) ||
+        !CU_OK(cudaEventCreateWithFlags(&side_.fork, cudaEventDisableTiming)) ||
+        !CU_OK(cudaEventCreateWithFlags(&side_.join, cudaEventDisableTiming))) {
+        cudaGetLastError();
+        destroy_side();
+    }
     host_results_cap_ = 256;
     if (!CU_OK(cudaMallocHost((void**)&host_results_, sizeof(TickResult) * host_results_cap_))) {
         cudaStreamDestroy(stream_);
@@ -72,6 +80,13 @@ pfsf_result Engine::init() {
     }
     available_ = true;
     return PFSF_OK;
+}
+
+void Engine::destroy_side() {
+    if (side_.stream) cudaStreamDestroy(side_.stream);
+    if (side_.fork) cudaEventDestroy(side_.fork);
+    if (side_.join) cudaEventDestroy(side_.join);
+    side_ = kappa::SideStream{nullptr, nullptr, nullptr};
 }
 
 void Engine::shutdown() {
@@ -83,6 +98,7 @@ void Engine::shutdown() {
     islands_.clear();
     if (host_results_) cudaFreeHost(host_results_);
     host_results_ = nullptr;
+    destroy_side();
     cudaStreamDestroy(stream_);
     stream_ = nullptr;
     vram_used_ = 0;

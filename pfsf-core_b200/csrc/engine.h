@@ -178,6 +178,7 @@ private:
     KArena solve_params(double tol, int32_t max_iter) const;
     pfsf_result run_solve(const KArena& k, std::vector<KDesc>& res, int64_t& launches);
     bool grid_barrier_failed() const;
+    void destroy_side();
     void fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_solve_stats& st) const;
     pfsf_result enqueue_tail(Island& isl, int32_t want_cap);
     pfsf_result finish_dispatch(const std::vector<Island*>& dispatched, bool drain, void* fail_addr, int32_t dbb_count,
@@ -198,6 +199,7 @@ private:
     bool available_ = false;
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
+    kappa::SideStream side_{nullptr, nullptr, nullptr};
     std::map<int32_t, std::unique_ptr<Island>> islands_;
     bool pcg_enabled_ = true;
     pfsf_vec3 wind_{0, 0, 0};
@@ -217,8 +219,8 @@ private:
     std::unique_ptr<Arena> arena_;
     int num_sms_ = 148;
     int64_t grid_min_voxels_ = 1 << 21;    // PFSF_GRID_MIN_VOXELS: whole-GPU tier
-    int64_t cluster_min_voxels_ = 131072;  // PFSF_CLUSTER_MIN_VOXELS
-    int cluster_size_ = 8;                // PFSF_CLUSTER (16, 8 or 1)
+    int64_t cluster_min_voxels_ = 262144;  // PFSF_CLUSTER_MIN_VOXELS
+    int cluster_size_ = 4;                // PFSF_CLUSTER (8, 4 or 1)
     int64_t warp_max_voxels_ = 0;         // PFSF_WARP_MAX_VOXELS (0: no warp tier)
     int smoother_ = -1;                   // PFSF_SMOOTHER (-1: mode default)
     int cheb_k_ = 3;                      // PFSF_CHEB_K

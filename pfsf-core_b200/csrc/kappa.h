@@ -110,13 +110,21 @@ struct KappaState {
 namespace kappa {
 // Plans levels for an island (host).
 int plan_levels(int lx, int ly, int lz, KLevel* lev);
+// A second stream and two events for the cluster-less launch that fills the
+// CTA slots a clustered launch leaves free (stream may be null: no fill).
+struct SideStream {
+    cudaStream_t stream;
+    cudaEvent_t fork, join;
+};
 // Batched solve over all islands in the arena: the first ngiant islands of
 // a.order are solved one at a time by a cooperative launch of the whole GPU,
-// the next nbig by thread-block clusters of `cluster` CTAs (16, 8 or 1) in
+// the next nbig by thread-block clusters of `cluster` CTAs (8, 4 or 1) in
 // one persistent launch, the last nsmall by single warps, the rest by single
-// CTAs.  a.queue[0..15] must be zero.  Returns 0 on success; a timed-out
-// grid barrier is reported later through a.queue[10] != 0.
-int launch_batched(cudaStream_t s, const KArena& a, int ngiant, int nbig, int nsmall, int cluster, int num_sms);
+// CTAs.  a.queue[0..15] must be zero.  Returns the CTAs of the persistent
+// launch(es) (kernel launches in *launches), -1 on a launch failure; a
+// timed-out grid barrier is reported later through a.queue[10] != 0.
+int launch_batched(cudaStream_t s, const SideStream& side, const KArena& a, int ngiant, int nbig, int nsmall,
+                   int cluster, int num_sms, int* launches);
 // Prepare kernels: sanitise kappa, round to 16-bit, zero non-solid source.
 void launch_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total, const int64_t* dummy);
 // Per-island plain solve driven from the host (one kernel per operation).

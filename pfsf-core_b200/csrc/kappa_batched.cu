@@ -630,8 +630,12 @@ cudaError_t launch_grid(cudaStream_t s, const KArena& a, int ngiant, int num_sms
     return cudaLaunchKernelEx(&cfg, kern, a, ngiant);
 }
 
+// k_batched with clusters of C CTAs: as many CTAs as can be resident (at
+// most max_ctas when > 0); *ctas = CTAs launched, *slots = CTAs the GPU could
+// hold without clusters.
 template <int P, int C>
-cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int nsmall, int num_sms) {
+cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int nsmall, int num_sms, int max_ctas,
+                       int* ctas_out, int* slots_out) {
     auto kern = k_batched<P, C>;
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
@@ -648,9 +652,9 @@ cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int 
         cudaGetLastError();
         per_sm = 1;
     }
+    *slots_out = num_sms * per_sm;
     int ctas = num_sms * per_sm;
     if (C > 1) {
-        if (C > 8) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = C;
         attr[0].val.clusterDim.y = 1;
@@ -668,27 +672,70 @@ cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int 
         cfg.attrs = nullptr;
         cfg.numAttrs = 0;
     }
+    if (max_ctas > 0) ctas = std::min(ctas, max_ctas);
     const int rest = std::max(1, a.nisl - base);
-    cfg.gridDim = dim3(std::max(C, std::min(ctas, std::max(C, rest * C))));
+    ctas = std::max(C, std::min(ctas, std::max(C, rest * C)));
+    cfg.gridDim = dim3(ctas);
+    *ctas_out = ctas;
     return cudaLaunchKernelEx(&cfg, kern, a, base, nbig, nsmall);
 }
 
+// Clusters of C CTAs cannot fill every CTA slot of a GPC (an 18-SM GPC
+// holds 36 CTAs of this kernel but only 4 clusters of 8), so the slots a
+// clustered launch leaves free get a second, cluster-less launch on the
+// side stream: it takes CTA- and warp-sized islands from the same queues
+// from the start.  Neither launch waits on the other (islands are handed
+// out by atomic counters), so they need not run at the same time.
+template <int P, int C>
+cudaError_t launch_clustered(cudaStream_t s, const SideStream& side, const KArena& a, int base, int nbig,
+                             int nsmall, int num_sms, int* ctas, int* launches) {
+    int used = 0, slots = 0;
+    cudaError_t e = launch_one<P, C>(s, a, base, nbig, nsmall, num_sms, 0, &used, &slots);
+    if (e != cudaSuccess) return e;
+    *ctas = used;
+    *launches = 1;
+    const int nmid = a.nisl - base - nbig - nsmall;
+    if (slots > used && side.stream && nmid + nsmall > 0) {
+        int used2 = 0, slots2 = 0;
+        if (cudaEventRecord(side.fork, s) != cudaSuccess || cudaStreamWaitEvent(side.stream, side.fork, 0) != cudaSuccess)
+            return cudaErrorLaunchFailure;
+        e = launch_one<P, 1>(side.stream, a, base, nbig, nsmall, num_sms, slots - used, &used2, &slots2);
+        if (e != cudaSuccess) return e;
+        if (cudaEventRecord(side.join, side.stream) != cudaSuccess || cudaStreamWaitEvent(s, side.join, 0) != cudaSuccess)
+            return cudaErrorLaunchFailure;
+        *ctas += used2;
+        *launches += 1;
+    }
+    return cudaSuccess;
+}
+
 template <int P>
-cudaError_t launch_p(cudaStream_t s, const KArena& a, int ngiant, int nbig, int nsmall, int cluster, int num_sms) {
+cudaError_t launch_p(cudaStream_t s, const SideStream& side, const KArena& a, int ngiant, int nbig, int nsmall,
+                     int cluster, int num_sms, int* ctas, int* launches) {
+    *ctas = 0;
+    *launches = 0;
     if (ngiant > 0) {
         const cudaError_t e = launch_grid<P>(s, a, ngiant, num_sms);
         if (e != cudaSuccess) return e;
+        *launches = 1;
         if (ngiant >= a.nisl) return cudaSuccess;
     }
-    if (nbig > 0 && cluster >= 16) {
-        if (launch_one<P, 16>(s, a, ngiant, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
+    int c = 0, l = 0;
+    cudaError_t e = cudaErrorInvalidConfiguration;
+    if (nbig > 0 && cluster >= 8) e = launch_clustered<P, 8>(s, side, a, ngiant, nbig, nsmall, num_sms, &c, &l);
+    if (e != cudaSuccess && nbig > 0 && cluster >= 4) {
         cudaGetLastError();
+        e = launch_clustered<P, 4>(s, side, a, ngiant, nbig, nsmall, num_sms, &c, &l);
     }
-    if (nbig > 0 && cluster >= 8) {
-        if (launch_one<P, 8>(s, a, ngiant, nbig, nsmall, num_sms) == cudaSuccess) return cudaSuccess;
+    if (e != cudaSuccess) {
         cudaGetLastError();
+        int slots = 0;
+        l = 1;
+        e = launch_one<P, 1>(s, a, ngiant, 0, nsmall, num_sms, 0, &c, &slots);
     }
-    return launch_one<P, 1>(s, a, ngiant, 0, nsmall, num_sms);
+    *ctas = c;
+    *launches += l;
+    return e;
 }
 
 }  // namespace
@@ -698,18 +745,20 @@ int batched_threads() { return kBatchedThreads; }
 // ngiant: leading islands (in a.order) solved by the whole grid; nbig: the
 // next ones, solved by whole clusters; nsmall: trailing islands solved by
 // single warps.
-int launch_batched(cudaStream_t s, const KArena& a, int ngiant, int nbig, int nsmall, int cluster, int num_sms) {
+int launch_batched(cudaStream_t s, const SideStream& side, const KArena& a, int ngiant, int nbig, int nsmall,
+                   int cluster, int num_sms, int* launches) {
     cudaError_t e;
+    int ctas = 0;
     switch (a.prec) {
-        case 1: e = launch_p<1>(s, a, ngiant, nbig, nsmall, cluster, num_sms); break;
-        case 2: e = launch_p<2>(s, a, ngiant, nbig, nsmall, cluster, num_sms); break;
-        default: e = launch_p<0>(s, a, ngiant, nbig, nsmall, cluster, num_sms); break;
+        case 1: e = launch_p<1>(s, side, a, ngiant, nbig, nsmall, cluster, num_sms, &ctas, launches); break;
+        case 2: e = launch_p<2>(s, side, a, ngiant, nbig, nsmall, cluster, num_sms, &ctas, launches); break;
+        default: e = launch_p<0>(s, side, a, ngiant, nbig, nsmall, cluster, num_sms, &ctas, launches); break;
     }
     if (e != cudaSuccess) {
         std::fprintf(stderr, "[libpfsf] batched solve launch failed: %s\n", cudaGetErrorString(e));
         return -1;
     }
-    return 0;
+    return ctas;
 }
 
 }  // namespace kappa

@@ -270,9 +270,12 @@ pfsf_result Engine::run_solve(const KArena& k, std::vector<KDesc>& res, int64_t&
             nbig += (d.n >= cluster_min_voxels_ && d.n < grid_min_voxels_) ? 1 : 0;
             nsmall += d.n < warp_max_voxels_ ? 1 : 0;
         }
-        if (kappa::launch_batched(stream_, k, ngiant, nbig, nsmall, cluster_size_, num_sms_) != 0)
-            return PFSF_ERROR_VULKAN;
-        nl = (ngiant > 0 ? 1 : 0) + (ngiant < (int)A.desc.size() ? 1 : 0);
+        int launches = 0;
+        const int ctas = kappa::launch_batched(stream_, side_, k, ngiant, nbig, nsmall, cluster_size_, num_sms_,
+                                               &launches);
+        if (ctas < 0) return PFSF_ERROR_VULKAN;
+        A.persistent_ctas = ctas;
+        nl = launches;
         int* flag = reinterpret_cast<int*>(A.hscratch) + 48;
         *flag = 0;
         cudaMemcpyAsync(flag, k.queue + 10, sizeof(int), cudaMemcpyDeviceToHost, stream_);
@@ -316,6 +319,7 @@ void Engine::fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_sol
             st.vcycle_tail_ms_sum += (double)d.t_vtail * 1e-6;
         }
         st.span_ms = t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
+        st.persistent_ctas = A.persistent_ctas;
     }
 }
 

@@ -88,7 +88,7 @@ class SolveStats(C.Structure):
                 ("active_voxels", C.c_int64), ("island_ms_sum", C.c_double), ("island_ms_max", C.c_double),
                 ("span_ms", C.c_double), ("setup_ms_sum", C.c_double), ("precond_ms_sum", C.c_double),
                 ("vcycle_fine_ms_sum", C.c_double), ("vcycle_coarse_ms_sum", C.c_double),
-                ("vcycle_tail_ms_sum", C.c_double)]
+                ("vcycle_tail_ms_sum", C.c_double), ("persistent_ctas", C.c_int32), ("reserved", C.c_int32)]
 
 
 class IslandReport(C.Structure):
