@@ -22,7 +22,10 @@ constexpr int kFlatThreads = 512;
 constexpr int kFlatMaxTX = 126;
 constexpr int kFlatZ = 16;  // planes per work item when several CTAs share an island
 __host__ __device__ inline void flat_tile(int lx, int ly, int& tx, int& ty) {
-    tx = lx <= kFlatMaxTX ? lx : kFlatMaxTX;
+    // wider islands: the fewest tiles of at most kFlatMaxTX columns, equal
+    // widths rounded up to even (no sliver tile at the far edge)
+    const int ntx = (lx + kFlatMaxTX - 1) / kFlatMaxTX;
+    tx = ntx <= 1 ? lx : ((((lx + ntx - 1) / ntx) + 1) & ~1);
     ty = (kFlatCap / (tx + 2) - 2) & ~1;
     if (ty >= ly) ty = ly;
 }

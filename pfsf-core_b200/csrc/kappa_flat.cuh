@@ -49,10 +49,10 @@ struct FlatGeom {
     int tx, ty, hx, hp, ntx, ntiles, zc, nwork;
 };
 // Tiles of the island, and work items of zc planes: the whole depth for a
-// single-CTA team; when ncta CTAs share the island, runs of planes long
-// enough that every CTA gets at most one work item if the tiles allow it
-// (each work item re-reads 3 planes, so runs stay at least kFlatZ / 2 long),
-// else kFlatZ.  zc is even, so plane pairs of one aggregate stay together.
+// single-CTA team; when ncta CTAs share the island, the run length that
+// minimises rounds x (zc + 3) plane steps for the busiest CTA (a work item
+// re-reads 3 planes), over runs of about kFlatZ / 2 planes and more.  zc is
+// even, so plane pairs of one aggregate stay together.
 __device__ __forceinline__ FlatGeom flat_geom(const KDesc& D, int ncta) {
     FlatGeom G;
     flat_tile(D.lx, D.ly, G.tx, G.ty);
@@ -63,8 +63,18 @@ __device__ __forceinline__ FlatGeom flat_geom(const KDesc& D, int ncta) {
     if (ncta == 1) {
         G.zc = D.lz;
     } else {
-        const int nz = ncta / G.ntiles;
-        G.zc = nz >= 1 ? max(kFlatZ / 2, (((D.lz + nz - 1) / nz) + 1) & ~1) : kFlatZ;
+        int best = 0x7fffffff;
+        G.zc = kFlatZ;
+        const int nzmax = max(1, D.lz / (kFlatZ / 2));
+        for (int nz = 1; nz <= nzmax; nz++) {
+            const int c = max(2, (((D.lz + nz - 1) / nz) + 1) & ~1);
+            const int rounds = (G.ntiles * ((D.lz + c - 1) / c) + ncta - 1) / ncta;
+            const int cost = rounds * (c + 3);
+            if (cost < best) {
+                best = cost;
+                G.zc = c;
+            }
+        }
     }
     G.nwork = G.ntiles * ((D.lz + G.zc - 1) / G.zc);
     return G;
