@@ -328,7 +328,9 @@ def run_ours(args):
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
     tm = traffic_model()
     traffic = None
-    if tm and tm.get("dram_bytes_per_active_voxel") and mode == capi.SOLVE_BATCHED:
+    # the committed capture is of k_batched; the whole-GPU tier (single workload)
+    # has no capture at a size whose working set exceeds L2, so no traffic figure
+    if tm and tm.get("dram_bytes_per_active_voxel") and mode == capi.SOLVE_BATCHED and args.workload == "batch":
         traffic = tm["dram_bytes_per_active_voxel"] * st0.active_voxels
     # FP64-oracle error on a few islands (read the FP64 accumulator back).
     # The single 256x256x128 island is too large for the CPU FP64 solve
