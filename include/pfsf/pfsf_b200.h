@@ -205,7 +205,9 @@ PFSF_API pfsf_result pfsf_label_components(pfsf_engine engine, const uint8_t* vo
  * 1 history H (float32 x N), 2 damage d (float32 x N), 3 failure flags
  * (uint8 x N), 4 macro-block residual bits (uint32 x blocks), 5 schedule state
  * {int32 chebyshev_iter, pcg_allocated, mg_allocated, float prev, last macro
- * residual} (20 bytes).  Copies min(bytes, field size); *out_bytes gets the
+ * residual} (20 bytes), and the device copies of the inputs: 6 source
+ * (float32 x N), 7 face conductivity (float32 x 6N, SoA), 8 voxel type
+ * (uint8 x N), 9 max_phi, 10 rcomp, 11 rtens (float32 x N).  Copies min(bytes, field size); *out_bytes gets the
  * field size. */
 PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine engine, int32_t island_id, int32_t field, void* out,
                                            int64_t bytes, int64_t* out_bytes);
@@ -227,13 +229,25 @@ PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine engine, int32_t island_id
  *   enqueues work, the caller synchronises before reading the outputs.
  * Limits and rules: islands above 67,108,864 voxels are rejected with
  * PFSF_ERROR_INVALID_ARG.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and caches it; make that
- * first call before any stream capture.  All calls on a device share the one
- * array, so calls whose GPU work overlaps (different streams, no ordering)
- * race and corrupt each other's results; serialise them. */
+ * array's device address (cudaGetSymbolAddress) and caches it together with
+ * the CUDA context current at the time; make that first call before any
+ * stream capture.  After cudaDeviceReset (a new primary context) the next
+ * call looks the address up again, so make that call outside a capture too.
+ * An error already pending in the CUDA runtime when the call starts (from the
+ * caller's own earlier work) is left pending and the call returns
+ * PFSF_ERROR_VULKAN without launching anything.  All calls on a device share
+ * the one array, so calls whose GPU work overlaps (different streams, no
+ * ordering) race and corrupt each other's results; serialise them. */
 PFSF_API pfsf_result pfsf_compact_failures_noalloc(const uint8_t* dev_fail_flags, int32_t lx, int32_t ly,
                                                    int32_t lz, pfsf_pos origin, int32_t* dev_tuples,
                                                    int32_t capacity, int32_t* dev_count, void* stream);
+
+/* Test access (no counterpart in the reference ABI): evaluates on the current
+ * device, for n host doubles s, the FP64 link reciprocal the tolerance solve
+ * uses (hardware reciprocal + two Newton steps; IEEE division outside
+ * [2^-1022, 2^1020]) into out_rcp64 and the IEEE quotient 1.0 / s into
+ * out_ieee.  Allocates its own device memory; n <= 2^26. */
+PFSF_API pfsf_result pfsf_debug_rcp64(const double* in, double* out_rcp64, double* out_ieee, int64_t n);
 
 /* The cudaStream_t the engine launches on (for event timing by callers). */
 PFSF_API void* pfsf_get_stream(pfsf_engine engine);

@@ -30,7 +30,7 @@
  * Arithmetic is FP32 in the order the shaders write it; the FP64 solve is
  * separate.  Where the reference is non-deterministic or reads out of
  * bounds, the restatement fixes one deterministic reading (documented at
- * each site and in DESIGN.md):
+ * each site):
  *   - jacobi_smooth binds phiPrev == phi (in-place, racy): restated as a
  *     Jacobi pass that reads a snapshot taken before the pass.
  *   - pcg_update reads neighbour r[j] while other workgroups rewrite it:

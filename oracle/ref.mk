@@ -10,7 +10,10 @@
 # reference's own build adds -march=x86-64-v3, whose FMA contraction the Java
 # side it mirrors does not have.  -Bsymbolic keeps the library's calls to
 # its own exports inside itself when it is loaded beside libpfsf.so.
-REF ?= /root/reference/L1-native/libpfsf
+# The reference checkout: PFSF_REFERENCE, else a directory named "reference"
+# beside this repository.
+PFSF_REFERENCE ?= $(abspath $(CURDIR)/../../reference)
+REF ?= $(PFSF_REFERENCE)/L1-native/libpfsf
 OUT := _ref
 CXX ?= g++
 CXXFLAGS := -O2 -std=c++17 -fPIC -ffp-contract=off -w -I$(REF)/include -DPFSF_ABI_VERSION_STRING='"1.5.0"'

@@ -666,6 +666,12 @@ pfsf_result Engine::debug_read_field(int32_t id, int32_t field, void* out, int64
         case 2: src = s->D; size = s->n * 4; break;
         case 3: src = s->fail; size = s->n; break;
         case 4: src = s->macro; size = s->nmb * 4; break;
+        case 6: src = s->src; size = s->n * 4; break;
+        case 7: src = s->sigma; size = s->n * 24; break;
+        case 8: src = s->type; size = s->n; break;
+        case 9: src = s->maxphi; size = s->n * 4; break;
+        case 10: src = s->rcomp; size = s->n * 4; break;
+        case 11: src = s->rtens; size = s->n * 4; break;
         default: return PFSF_ERROR_INVALID_ARG;
     }
     *out_bytes = size;

@@ -84,11 +84,15 @@ __device__ __forceinline__ float hm(float a, float b) {
 }
 // 1/s for s > 0: the hardware approximation (rcp.approx.ftz.f64, about 2^-23
 // relative) refined by two Newton steps r <- r + r(1 - s r), each squaring
-// the relative error, to within an ulp or two of the correctly rounded
-// quotient -- far below what the FP64 residual needs (link weights to
-// ~1e-12).  The FP64 residual pass measured 2.7x faster than with IEEE
-// double division, its FP32 output bitwise unchanged on the probe islands.
+// the relative error, to within an ulp of the correctly rounded quotient --
+// far below what the FP64 residual needs (link weights to ~1e-12).  The FP64
+// residual pass measured 2.7x faster than with IEEE double division.  The
+// approximation flushes subnormal inputs (1/s = inf, and the Newton step
+// then gives NaN) and subnormal results (s near DBL_MAX gives 0), so s
+// outside [2^-1022, 2^1020] takes the IEEE division; kappa sums of the solve
+// (kappa normalised to mean 1) never get near either end.
 __device__ __forceinline__ double rcp64(double s) {
+    if (!(s >= 0x1p-1022 && s <= 0x1p+1020)) return 1.0 / s;
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
     double e = fma(-s, r, 1.0);

@@ -12,6 +12,7 @@
 // point runs the same compaction with its scratch in a file-scope device
 // array instead, so the only memory it touches is the caller's input and
 // output buffers plus that fixed array.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -31,21 +32,54 @@ constexpr int kMaxDevices = 64;
 // every GPU that loads the library, held until the process exits.
 static __device__ __align__(256) int32_t g_compact_scratch[2 * kNoAllocMaxChunks];
 
+// The address is cached per device together with the CUDA context it was
+// looked up in: after cudaDeviceReset (or any teardown of the primary
+// context) the module is loaded again at another address, so a cached
+// address is only reused while the same context is current.
+struct ScratchSlot {
+    CUcontext ctx;
+    int32_t* addr;
+};
 std::mutex g_setup_mutex;
-int32_t* g_scratch_addr[kMaxDevices] = {};
+ScratchSlot g_slots[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+// The calling thread's current context (nullptr when none is current or the
+// driver entry point is unavailable), through the runtime's driver entry
+// point query, so the library needs no link against libcuda.
+CUcontext current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<CtxGetCurrentFn>(nullptr);
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 
 // Device address of g_compact_scratch on the current device.  The host-side
 // symbol is only a stand-in for the device array, so the address is looked up
-// once per device, with that device current, and cached.
+// with that device current (cudaGetSymbolAddress) and cached for the context
+// it was found in.
 cudaError_t scratch_address(int device, int32_t** out) {
     std::lock_guard<std::mutex> lk(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
+    ScratchSlot& slot = g_slots[device];
+    const CUcontext ctx = current_context();
+    if (!slot.addr || !ctx || slot.ctx != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_compact_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_addr[device] = static_cast<int32_t*>(p);
+        slot.addr = static_cast<int32_t*>(p);
+        slot.ctx = current_context();  // the lookup makes the primary context current
     }
-    *out = g_scratch_addr[device];
+    *out = slot.addr;
     return cudaSuccess;
 }
 
@@ -66,6 +100,9 @@ extern "C" PFSF_API pfsf_result pfsf_compact_failures_noalloc(const uint8_t* dev
                      (long long)n, (long long)(kNoAllocMaxChunks * 4096));
         return PFSF_ERROR_INVALID_ARG;
     }
+    // An error still pending from the caller's own earlier work is not this
+    // call's: report it without clearing it and launch nothing.
+    if (cudaPeekAtLastError() != cudaSuccess) return PFSF_ERROR_VULKAN;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) {
         cudaGetLastError();

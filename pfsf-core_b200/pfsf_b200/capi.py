@@ -1,7 +1,7 @@
 """ctypes binding of libpfsf.so (the C ABI in include/pfsf/*.h).
 
 This is the binding a Python caller -- or a test -- uses; the Java caller
-binds the same symbols through JNI.  Loading fails
+binds the same symbols through a JNI shim.  Loading fails
 loudly when the library has not been built: there is no fallback path.
 """
 from __future__ import annotations
@@ -153,6 +153,7 @@ def load():
         "pfsf_debug_read_field": ([E, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
         "pfsf_compact_failures_noalloc": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, Pos, C.c_void_p, C.c_int32,
                                            C.c_void_p, C.c_void_p], C.c_int),
+        "pfsf_debug_rcp64": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
     }
@@ -291,11 +292,13 @@ class Engine:
         rc = self.L.pfsf_read_stress(self.h, iid, _ptr(out), n, C.byref(cnt))
         return rc, out[:cnt.value]
 
-    FIELD_DTYPES = {0: np.float32, 1: np.float32, 2: np.float32, 3: np.uint8, 4: np.uint32}
+    FIELD_DTYPES = {0: np.float32, 1: np.float32, 2: np.float32, 3: np.uint8, 4: np.uint32, 6: np.float32,
+                    7: np.float32, 8: np.uint8, 9: np.float32, 10: np.float32, 11: np.float32}
 
     def debug_field(self, iid, field):
-        """Tick-state array of an island (0 phi, 1 H, 2 d, 3 fail, 4 macro bits) or
-        the schedule state dict (field 5)."""
+        """Tick-state array of an island (0 phi, 1 H, 2 d, 3 fail, 4 macro bits,
+        6 source, 7 face conductivity SoA-6, 8 type, 9 max_phi, 10 rcomp,
+        11 rtens) or the schedule state dict (field 5)."""
         size = C.c_int64(0)
         tmp = np.zeros(32, np.uint8)
         rc = self.L.pfsf_debug_read_field(self.h, iid, field, _ptr(tmp), 0, C.byref(size))

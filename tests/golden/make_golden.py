@@ -63,7 +63,8 @@ def ticks():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PFSF_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference")),
+                    help="reference checkout (default: $PFSF_REFERENCE, else ../reference beside this repository)")
     a = ap.parse_args()
     if os.path.isdir(a.reference):
         fx = fixtures(a.reference)

@@ -186,17 +186,64 @@ def test_not_dirty_island_is_skipped(eng):
 
 
 def test_sparse_scatter_updates_device_arrays(eng):
-    case = cases.compat_case("block8")
-    iid, host, ref = _setup(eng, case)
+    """48-byte records (SH/sparse_scatter.comp.glsl:47-66: flat index, source,
+    type, maxPhi, rcomp, rtens, six face conductivities in SoA order) land in
+    the device arrays; out-of-island indices are skipped; the island is marked
+    dirty and the next tick -- which, as in the reference, re-uploads the
+    caller's arrays, kept in step with the edits -- matches the oracle run on
+    the edited inputs."""
     import ctypes as C
+    case = cases.compat_case("noise20")
+    origin = (3, -2, 7)
+    iid, host, ref = _setup(eng, case, origin)
+    fb, want = _tick_both(eng, iid, host, ref, origin)
+    _assert_tick_parity(eng, iid, host, ref, fb, want, 0)
+    n = int(np.prod(case["dims"]))
     addr = C.c_void_p()
     nbytes = C.c_int64()
     assert eng.L.pfsf_get_sparse_upload_buffer(eng.h, iid, C.byref(addr), C.byref(nbytes)) == capi.PFSF_OK
     assert nbytes.value == 512 * 48
-    rec = np.frombuffer((C.c_byte * nbytes.value).from_address(addr.value), dtype=np.uint32)
-    rec[:12] = 0
-    rec[0] = 5
-    rec[1:2] = np.array([0.25], np.float32).view(np.uint32)
-    rec[2] = 1
-    assert eng.L.pfsf_notify_sparse_updates(eng.h, iid, 1) == capi.PFSF_OK
+    rec = np.frombuffer((C.c_byte * nbytes.value).from_address(addr.value), dtype=np.uint32).reshape(512, 12)
+    rng = np.random.default_rng(21)
+    idx = rng.choice(n, 40, replace=False)
+    src = rng.uniform(0.0, 3.0, idx.size).astype(np.float32)
+    vt = rng.integers(0, 3, idx.size).astype(np.uint32)
+    mphi = rng.uniform(5.0, 50.0, idx.size).astype(np.float32)
+    rc_ = rng.uniform(0.5, 40.0, idx.size).astype(np.float32)
+    rt_ = rng.uniform(0.1, 5.0, idx.size).astype(np.float32)
+    cond = rng.uniform(0.0, 1.0, (idx.size, 6)).astype(np.float32)
+    cond[vt == 0] = 0.0
+    rec[:] = 0
+    rec[: idx.size, 0] = idx
+    rec[: idx.size, 1] = src.view(np.uint32)
+    rec[: idx.size, 2] = vt
+    rec[: idx.size, 3] = mphi.view(np.uint32)
+    rec[: idx.size, 4] = rc_.view(np.uint32)
+    rec[: idx.size, 5] = rt_.view(np.uint32)
+    rec[: idx.size, 6:] = cond.view(np.uint32)
+    # two records outside the island: skipped
+    rec[idx.size: idx.size + 2, 0] = [n, n + 1000]
+    rec[idx.size: idx.size + 2, 1:] = np.float32(123.0).view(np.uint32)
+    # the Java side keeps its zero-copy arrays in step with the edits it scatters
+    host["source"][idx] = src
+    host["type"][idx] = vt.astype(np.uint8)
+    host["max_phi"][idx] = mphi
+    host["rcomp"][idx] = rc_
+    host["rtens"][idx] = rt_
+    cv = host["conductivity"].reshape(-1)
+    for d in range(6):
+        cv[d * n + idx] = cond[:, d]
+    assert eng.L.pfsf_notify_sparse_updates(eng.h, iid, idx.size + 2) == capi.PFSF_OK
     assert eng.L.pfsf_notify_sparse_updates(eng.h, iid, 0) == capi.PFSF_OK
+    for field, name, dt in ((6, "source", np.float32), (7, "conductivity", np.float32), (8, "type", np.uint8),
+                            (9, "max_phi", np.float32), (10, "rcomp", np.float32), (11, "rtens", np.float32)):
+        dev = eng.debug_field(iid, field)
+        want_arr = np.ascontiguousarray(host[name]).reshape(-1).astype(dt)
+        assert np.array_equal(dev.view(np.uint8), want_arr.view(np.uint8)), f"device {name} after scatter"
+    # the edit marked the island dirty: the next tick runs on the edited inputs
+    ref.load(source=host["source"], conductivity=host["conductivity"], type=host["type"], rcomp=host["rcomp"],
+             rtens=host["rtens"], max_phi=host["max_phi"])
+    for t in range(1, 3):
+        fb, want = _tick_both(eng, iid, host, ref, origin)
+        _assert_tick_parity(eng, iid, host, ref, fb, want, t)
+        eng.L.pfsf_mark_full_rebuild(eng.h, iid)

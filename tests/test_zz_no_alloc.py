@@ -61,6 +61,26 @@ def test_noalloc_compaction_matches_tick_failure_buffer(lib_built):
         np.testing.assert_array_equal(got[: 4 * count], fb[1: 1 + 4 * count])
         assert np.all(got[4 * count:] == -7)
 
+    # a buffer smaller than the failure count: *dev_count is still the full
+    # count, the first `small` tuples are written, nothing past them; on a
+    # non-default stream the caller orders its reads after the stream
+    small = count // 3
+    assert small > 0
+    side = torch.cuda.Stream(device=dev)
+    for rep in range(2):
+        d_tuples.fill_(-7)
+        d_count.fill_(-1)
+        torch.cuda.synchronize()
+        rc = eng.L.pfsf_compact_failures_noalloc(C.c_void_p(d_fail.data_ptr()), lx, ly, lz, capi.Pos(*origin),
+                                                 C.c_void_p(d_tuples.data_ptr()), small,
+                                                 C.c_void_p(d_count.data_ptr()), C.c_void_p(side.cuda_stream))
+        assert rc == capi.PFSF_OK
+        side.synchronize()
+        assert int(d_count.cpu().item()) == count
+        got = d_tuples.cpu().numpy()
+        np.testing.assert_array_equal(got[: 4 * small], fb[1: 1 + 4 * small])
+        assert np.all(got[4 * small:] == -7), f"call {rep}: tuples written past the capacity"
+
     # sizes beyond the fixed scratch are rejected, nothing is launched
     rc = eng.L.pfsf_compact_failures_noalloc(C.c_void_p(d_fail.data_ptr()), 4096, 4096, 8, capi.Pos(0, 0, 0),
                                              C.c_void_p(d_tuples.data_ptr()), cap, C.c_void_p(d_count.data_ptr()),
