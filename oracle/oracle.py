@@ -33,8 +33,8 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(_HERE, "pfsf_oracle.c")
-        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        srcs = [os.path.join(_HERE, f) for f in ("pfsf_oracle.c", "kappa_mg.c", "kappa_mg_impl.h", "Makefile")]
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(_LIB_PATH)
         i = C.c_int
@@ -69,6 +69,11 @@ def lib():
         L.o_kappa_apply.argtypes = [i, i, i, F64P, U8P, F64P, F64P]
         L.o_kappa_pcg64.argtypes = [i, i, i, F64P, U8P, F64P, F64P, C.c_double, i, C.POINTER(C.c_double)]
         L.o_kappa_pcg64.restype = i
+        L.o_kappa_mgpcg64.argtypes = [i, i, i, F64P, U8P, F64P, F64P, C.c_double, i, i, C.POINTER(C.c_double)]
+        L.o_kappa_mgpcg64.restype = i
+        L.o_kappa_mgpcg32.argtypes = [i, i, i, F64P, U8P, F64P, F64P, C.c_double, i, i, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_int)]
+        L.o_kappa_mgpcg32.restype = i
         L.o_kappa_relres.argtypes = [i, i, i, F64P, U8P, F64P, F32P]
         L.o_kappa_relres.restype = C.c_double
         L.o_history.argtypes = [i, i, i, F32P, F32P, U8P, F32P]
@@ -257,6 +262,31 @@ def kappa_solve64(dims, kappa, vtype, source, tol=1e-12, maxit=20000, x0=None):
     it = lib().o_kappa_pcg64(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(source, np.float64), x,
                              float(tol), int(maxit), C.byref(rr))
     return x, it, rr.value
+
+
+def kappa_mgpcg64(dims, kappa, vtype, source, tol=1e-12, maxit=2000, threads=1, x0=None):
+    """FP64 multigrid-preconditioned CG (oracle/kappa_mg.c) on the same
+    operator: the FP64 reference solution of large islands in seconds to
+    minutes on the host's threads.  Returns (x, iterations, relres)."""
+    n = int(np.prod(dims))
+    x = np.zeros(n, np.float64) if x0 is None else np.array(x0, np.float64)
+    rr = C.c_double(0.0)
+    it = lib().o_kappa_mgpcg64(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(source, np.float64), x,
+                               float(tol), int(maxit), int(threads), C.byref(rr))
+    return x, it, rr.value
+
+
+def kappa_mgpcg32(dims, kappa, vtype, source, tol=1e-6, maxit=2000, threads=1, x0=None):
+    """The plain FP32 scheme on the CPU (oracle/kappa_mg.c): FP32 V-cycle PCG
+    inside FP64 residual refinement.  Returns (x, inner iterations, relres,
+    outer refinements)."""
+    n = int(np.prod(dims))
+    x = np.zeros(n, np.float64) if x0 is None else np.array(x0, np.float64)
+    rr = C.c_double(0.0)
+    outer = C.c_int(0)
+    it = lib().o_kappa_mgpcg32(*dims, _c(kappa, np.float64), _c(vtype, np.uint8), _c(source, np.float64), x,
+                               float(tol), int(maxit), int(threads), C.byref(rr), C.byref(outer))
+    return x, it, rr.value, outer.value
 
 
 def kappa_relres(dims, kappa, vtype, source, phi32):
