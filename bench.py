@@ -119,41 +119,83 @@ def stratified(isls, k):
     return [order[int(j * step)] for j in range(k)]
 
 
-def cpu_baseline(isls, seconds, tol):
-    """The oracle's FP64 Jacobi-PCG solve (oracle/pfsf_oracle.c o_kappa_pcg64)
-    on a size-stratified sample of islands, one island per host thread,
-    scaled to the whole tick by island count."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import concurrent.futures as cf
-    import oracle as O
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
     O.lib()
+    return O
+
+
+def cpu_solve_islands(isls, idx, tol, threads):
+    """Solves islands idx with the oracle's plain FP32 scheme (FP32 V-cycle
+    PCG inside FP64 residual refinement, oracle/kappa_mg.c o_kappa_mgpcg32) on
+    `threads` host threads: islands larger than half a thread's share of the
+    set first, one at a time, each threaded across all host threads (OpenMP
+    inside the solve); the rest one island per thread, largest first.
+    Returns (wall s, [(island, seconds, threads used)], islands converged)."""
+    import concurrent.futures as cf
+    O = _oracle()
+    order = sorted(idx, key=lambda i: -isls[i].n)
+    share = sum(isls[i].n for i in order) / max(threads, 1)
+    big = [i for i in order if threads > 1 and isls[i].n > share / 2]
+    rest = [i for i in order if i not in set(big)]
+
+    def run(i, nt):
+        s = isls[i]
+        t0 = time.perf_counter()
+        _, _, rel, _ = O.kappa_mgpcg32(s.dims, s.kappa.astype(np.float64), s.vtype, s.source.astype(np.float64),
+                                       tol=tol, maxit=100000, threads=nt)
+        return i, time.perf_counter() - t0, nt, rel <= tol
+
+    t0 = time.perf_counter()
+    res = [run(i, threads) for i in big]
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        res += list(ex.map(lambda i: run(i, 1), rest))
+    wall = time.perf_counter() - t0
+    return wall, [(r[0], r[1], r[2]) for r in res], sum(r[3] for r in res)
+
+
+def cpu_baseline(isls, seconds, tol):
+    """The plain FP32 scheme on the host cores (cpu_solve_islands), on an
+    interleaved sample of the tick's islands (every m-th island in size order,
+    so every size is represented), m chosen from a calibration solve so the
+    sample takes about `seconds` on all threads.  The tick estimate scales the
+    sample's wall time by grid voxels (the CPU passes sweep every cell of an
+    island's box): all threads = wall x N_all / N_sample; one thread = the
+    single-threaded per-island times of the sample, per grid voxel, x N_all."""
     threads = os.cpu_count() or 1
     order = sorted(range(len(isls)), key=lambda i: -isls[i].n)
-    # grow the sample (evenly spaced in size order) until the CPU budget is used
-    k = max(threads, 8)
-    t_used = 0.0
-    done = 0
-    while True:
-        sample = stratified(isls, min(k, len(isls)))
-
-        def run(i):
-            s = isls[i]
-            O.kappa_solve64(s.dims, s.kappa.astype(np.float64), s.vtype, s.source.astype(np.float64), tol=tol,
-                            maxit=200000)
-
-        t0 = time.perf_counter()
-        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-            list(ex.map(run, sample))
-        t_used = time.perf_counter() - t0
-        done = len(sample)
-        if t_used * 2 > seconds or done >= len(isls):
-            break
-        k = min(len(isls), k * 2)
-    ms = t_used * 1000.0 * len(isls) / done
-    return {"value": ms, "unit": "ms/tick", "cores": threads, "kind": "port",
-            "sample": f"{done} of {len(isls)} islands (size-stratified), FP64 Jacobi-PCG to {tol:g}, "
-                      f"{t_used:.1f} s wall on {threads} threads, scaled by island count"}
+    n_all = float(sum(i.n for i in isls))
+    # calibration: the island at the 25th size percentile
+    cal = order[len(order) // 4]
+    _, tc, _ = cpu_solve_islands(isls, [cal], tol, 1)
+    est_1t = tc[0][1] / isls[cal].n * n_all  # whole tick on one thread
+    m = max(1, int(est_1t / threads / max(seconds, 1.0)))
+    sample = order[m // 2::m] if (m > 1 and len(order) >= 2 * m) else order
+    wall, recs, conv = cpu_solve_islands(isls, sample, tol, threads)
+    n_s = float(sum(isls[i].n for i in sample))
+    one = [(isls[i].n, t) for i, t, nt in recs if nt == 1]
+    one_ms = (sum(t for _, t in one) / sum(n for n, _ in one) * n_all * 1000.0) if one else None
+    return {"value": wall * 1000.0 * n_all / n_s, "unit": "ms/tick", "cores": threads, "kind": "port",
+            "one_thread_ms": one_ms, "cpu": cpu_model(),
+            "sample": (f"every {m}th island in size order: {len(sample)} of {len(isls)} islands, "
+                       f"{n_s / n_all:.4f} of the grid voxels, {wall:.1f} s wall on {threads} threads, scaled by "
+                       f"grid voxels; one-thread figure from the sample's single-threaded island times per grid "
+                       f"voxel; converged {conv}/{len(sample)}"),
+            "algorithm": (f"plain FP32 scheme on the host (oracle/kappa_mg.c): 8-colour RBGS V-cycle PCG in FP32 "
+                          f"inside FP64 residual refinement, to {tol:g} FP64 relative residual; islands above half a "
+                          f"thread's share threaded across all cores, the rest one per thread")}
 
 
 class Clocks:
@@ -225,24 +267,46 @@ def traffic_model():
 
 
 def run_reference(args):
+    """The reference arm: the CPU scheme on the host cores for the same
+    workload.  The K timed steps partition the tick's islands (step j takes
+    every K-th island in size order from offset j), so together they solve
+    every island of one tick once: value = the sum of the step times = one
+    whole tick, measured; each step is a bounded, representative slice.
+    Warm-up steps solve the 16 smallest islands."""
     ws, rank, _ = dist_info()
     if rank != 0:
         return
     isls, meta = make_workload(args, 0)
-    vals = []
-    cb = None
-    # each step is a bounded, size-stratified sample of the tick (see cpu_baseline)
-    for _ in range(max(args.steps, 1)):
-        cb = cpu_baseline(isls, args.cpu_seconds, args.tol)
-        vals.append(cb["value"])
-    v = float(np.mean(vals))
-    cb["value"] = v
-    line = {"metric": METRIC, "value": v, "unit": "ms/tick", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"{len(isls)} islands, {meta['active_total']} active voxels, tol {args.tol:g}",
-                       "islands": len(isls), "active_voxels": meta["active_total"]},
-            "cpu_baseline": cb, "e2e": {"value": v, "unit": "ms/tick", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    threads = os.cpu_count() or 1
+    order = sorted(range(len(isls)), key=lambda i: -isls[i].n)
+    for _ in range(args.warmup):
+        cpu_solve_islands(isls, order[-16:], args.tol, threads)
+    k = max(args.steps, 1)
+    times, conv, cpu_s = [], 0, 0.0
+    for j in range(k):
+        wall, recs, c = cpu_solve_islands(isls, order[j::k], args.tol, threads)
+        times.append(wall * 1000.0)
+        conv += c
+        cpu_s += sum(t * nt for _, t, nt in recs)
+    tick_ms = float(sum(times))
+    cb = {"value": tick_ms, "unit": "ms/tick", "cores": threads, "kind": "port", "cpu": cpu_model(),
+          "thread_seconds": cpu_s,
+          "sample": (f"the whole tick: {len(isls)} islands split over {k} timed steps (every {k}th island in size "
+                     f"order); islands above half a thread's share threaded across all cores, the rest one per "
+                     f"thread, largest first; converged {conv}/{len(isls)}"),
+          "algorithm": (f"plain FP32 scheme on the host (oracle/kappa_mg.c): 8-colour RBGS V-cycle PCG in FP32 "
+                        f"inside FP64 residual refinement, to {args.tol:g} FP64 relative residual")}
+    line = {"metric": METRIC, "value": tick_ms, "unit": "ms/tick", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": float(np.mean(times)), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": (f"{len(isls)} islands (log-uniform sides, scale {meta['scale']:.3f}), "
+                                    f"{meta['grid_total']} grid / {meta['active_total']} active voxels, cold start, "
+                                    f"tol {args.tol:g}"),
+                       "islands": len(isls), "grid_voxels": meta["grid_total"],
+                       "active_voxels": meta["active_total"],
+                       "step": "1/K of the tick's islands; value = sum over the K steps = one tick"},
+            "cpu_baseline": cb,
+            "e2e": {"value": tick_ms, "unit": "ms/tick", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -332,31 +396,44 @@ def run_ours(args):
     # has no capture at a size whose working set exceeds L2, so no traffic figure
     if tm and tm.get("dram_bytes_per_active_voxel") and mode == capi.SOLVE_BATCHED and args.workload == "batch":
         traffic = tm["dram_bytes_per_active_voxel"] * st0.active_voxels
-    # FP64-oracle error on a few islands (read the FP64 accumulator back).
-    # The single 256x256x128 island is too large for the CPU FP64 solve
-    # (hours single-threaded); for it the oracle evaluates the relative
-    # residual of the returned FP64 solution with its own FP64 operator.
+    # FP64-oracle error (read the FP64 accumulator back): the oracle's FP64
+    # multigrid CG (all host threads) solves the same island to 1e-11; for
+    # the batch, 4 islands evenly spaced in size order (the largest included)
     oracle_err = None
     oracle_relres = None
     if rank == 0:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
+        O = _oracle()
         errs, rels = [], []
         for k in stratified(isls, 4):
             isl = isls[k]
             rc, x64 = eng.read_solution64(ids[k], isl.n)
             k64 = isl.kappa.astype(np.float64)
-            r = isl.source.astype(np.float64) - O.kappa_apply(isl.dims, k64, isl.vtype, x64)
+            s64 = isl.source.astype(np.float64)
+            r = s64 - O.kappa_apply(isl.dims, k64, isl.vtype, x64)
             solid = isl.vtype == 1
-            rels.append(float(np.linalg.norm(r[solid]) / np.linalg.norm(isl.source[solid].astype(np.float64))))
-        oracle_relres = max(rels)
-        for k in ([] if args.workload == "single" else stratified(isls, 4)):
-            isl = isls[k]
-            rc, x64 = eng.read_solution64(ids[k], isl.n)
-            xr, _, _ = O.kappa_solve64(isl.dims, isl.kappa.astype(np.float64), isl.vtype,
-                                       isl.source.astype(np.float64), tol=1e-12, maxit=200000)
+            rels.append(float(np.linalg.norm(r[solid]) / np.linalg.norm(s64[solid])))
+            xr, _, _ = O.kappa_mgpcg64(isl.dims, k64, isl.vtype, s64, tol=1e-11, maxit=5000,
+                                       threads=os.cpu_count() or 1)
             errs.append(float(np.abs(x64 - xr).max() / max(np.abs(xr).max(), 1e-300)))
-        oracle_err = max(errs) if errs else None
+        oracle_relres = max(rels)
+        oracle_err = max(errs)
+    # the same persistent kernel with FP32 kappa / coarse storage: isolates
+    # what the 16-bit storage contributes
+    fp32_ms = None
+    if args.precision != "fp32" and not args.no_plain and rank == 0:
+        eng.set_solve_mode(capi.SOLVE_BATCHED)
+        eng.set_precision(capi.PREC_FP32)
+        eng.solve(ids, tol=args.tol, flags=capi.SOLVE_COLD_START)  # rebuilds the arena for FP32 storage
+        ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev2.record(stream)
+        nrep = max(1, min(args.steps, 5))
+        for _ in range(nrep):
+            rc, st32 = eng.solve(ids, tol=args.tol, flags=resident)
+        ev3.record(stream)
+        torch.cuda.synchronize()
+        fp32_ms = ev2.elapsed_time(ev3) / nrep
+        fp32_conv = st32.islands_converged
     # plain FP32 per-island kernels on a stratified sample
     plain_ms = None
     plain_note = None
@@ -372,7 +449,7 @@ def run_ours(args):
                       f"converged {stp.islands_converged}/{len(sample)}, scaled by island count")
     # the CPU FP64 solve of the single 5 M-voxel island does not fit a bounded sample
     cb = (cpu_baseline(isls, args.cpu_seconds, args.tol)
-          if (rank == 0 and ws == 1 and not args.no_cpu and args.workload == "batch") else None)
+          if (rank == 0 and ws == 1 and not args.no_cpu) else None)
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": "ms/tick", "n_gpus": ws, "steps": args.steps,
@@ -391,6 +468,12 @@ def run_ours(args):
             "e2e": {"value": e2e_ms, "unit": "ms/tick", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "dram_gbs": (traffic / (kern_ms * 1e-3) / 1e9) if traffic else None,
+                         "dram_frac": (traffic / (kern_ms * 1e-3) / 1e9 / peak) if traffic else None,
+                         "note": ("achieved/frac: the engine's byte model (every array a pass touches counted "
+                                  "once per pass) over the kernel time; dram_gbs/dram_frac: DRAM bytes from the "
+                                  "committed ncu capture scaled to this workload over the same time -- islands "
+                                  "stay L2-resident while their team solves them"),
                          "kernel": ("k_batched (persistent solve)" if args.workload == "batch"
                                     else "k_grid (whole-GPU persistent solve)"), "kernel_ms": kern_ms,
                          "algorithmic_bytes": alg_bytes},
@@ -401,6 +484,9 @@ def run_ours(args):
             "fp64_oracle_error": oracle_err, "fp64_oracle_relres": oracle_relres,
             "plain_fp32_ms_per_tick": plain_ms, "plain_fp32_sample": plain_note,
             "speedup_vs_plain_fp32": (plain_ms / ms) if plain_ms else None,
+            "batched_fp32_ms_per_tick": fp32_ms,
+            "batched_fp32_converged": (f"{fp32_conv}/{len(isls)}" if fp32_ms else None),
+            "speedup_vs_batched_fp32": (fp32_ms / ms) if fp32_ms else None,
             "inner_iterations_total": int(stats[-1].inner_iterations_total),
             "schedule": {"island_ms_sum": stats[-1].island_ms_sum, "island_ms_max": stats[-1].island_ms_max,
                          "span_ms": stats[-1].span_ms, "setup_ms_sum": stats[-1].setup_ms_sum,
