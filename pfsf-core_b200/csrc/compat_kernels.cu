@@ -99,16 +99,14 @@ __device__ __forceinline__ void load_s6(const float* __restrict__ sigma, int64_t
 
 // ---------------------------------------------------------------- RBGS colour
 // SH/rbgs_smooth.comp.glsl:73-211.  One thread per voxel of colour `color`.
-__global__ void __launch_bounds__(kBlock) k_rbgs_color(int lx, int ly, int lz, float* __restrict__ phi,
-                                                       const float* __restrict__ rho,
-                                                       const float* __restrict__ sigma,
-                                                       const uint8_t* __restrict__ type, float* __restrict__ H,
-                                                       const uint32_t* __restrict__ macro, int color,
-                                                       float damping) {
+__device__ __forceinline__ void d_rbgs_color(int lx, int ly, int lz, float* __restrict__ phi,
+                                             const float* __restrict__ rho, const float* __restrict__ sigma,
+                                             const uint8_t* __restrict__ type, float* __restrict__ H,
+                                             const uint32_t* __restrict__ macro, int color, float damping,
+                                             int64_t t) {
     const int cx = color & 1, cy = (color >> 1) & 1, cz = (color >> 2) & 1;
     const int ncx = (lx - cx + 1) >> 1, ncy = (ly - cy + 1) >> 1, ncz = (lz - cz + 1) >> 1;
     const int64_t nc = (int64_t)ncx * ncy * ncz;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nc) return;
     const int xi = (int)(t % ncx);
     const int64_t rem = t / ncx;
@@ -136,17 +134,26 @@ __global__ void __launch_bounds__(kBlock) k_rbgs_color(int lx, int ly, int lz, f
     if (isnan(result)) result = phi[i];
     phi[i] = result;
 }
+__global__ void __launch_bounds__(kBlock) k_rbgs_color(int lx, int ly, int lz, float* __restrict__ phi,
+                                                       const float* __restrict__ rho,
+                                                       const float* __restrict__ sigma,
+                                                       const uint8_t* __restrict__ type, float* __restrict__ H,
+                                                       const uint32_t* __restrict__ macro, int color,
+                                                       float damping) {
+    d_rbgs_color(lx, ly, lz, phi, rho, sigma, type, H, macro, color, damping,
+                 (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 
 // ---------------------------------------------------------------- history
 // H = max(H, psi_e(phi)) on solid voxels with phi > 0 -- the history update
 // the reference performs inside every RBGS / Jacobi sweep
 // (SH/rbgs_smooth.comp.glsl:177-191), applied once to a given phi (the
 // tolerance tick, whose phi does not come from sweeps).
-__global__ void __launch_bounds__(kBlock) k_history(int lx, int ly, int lz, const float* __restrict__ phi,
-                                                    const float* __restrict__ sigma,
-                                                    const uint8_t* __restrict__ type, float* __restrict__ H) {
+__device__ __forceinline__ void d_history(int lx, int ly, int lz, const float* __restrict__ phi,
+                                          const float* __restrict__ sigma, const uint8_t* __restrict__ type,
+                                          float* __restrict__ H, int64_t i) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || type[i] != kSolid) return;
     const float p = phi[i];
     if (!(p > 0.0f)) return;
@@ -160,19 +167,21 @@ __global__ void __launch_bounds__(kBlock) k_history(int lx, int ly, int lz, cons
     }
     H[i] = fmaxf(H[i], amor_psi(s6, nphi6, x, y, z, lx, ly, lz, p));
 }
+__global__ void __launch_bounds__(kBlock) k_history(int lx, int ly, int lz, const float* __restrict__ phi,
+                                                    const float* __restrict__ sigma,
+                                                    const uint8_t* __restrict__ type, float* __restrict__ H) {
+    d_history(lx, ly, lz, phi, sigma, type, H, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // ---------------------------------------------------------------- coarse Jacobi
 // SH/jacobi_smooth.comp.glsl:60-227, omega = 1, reading phi_in (a snapshot)
 // and writing every voxel of phi_out.  Hfine is the fine-level history buffer,
 // which the reference binds at every level (coarse cell i updates Hfine[i]).
-__global__ void __launch_bounds__(kBlock) k_jacobi_coarse(int lx, int ly, int lz, float* __restrict__ phi_out,
-                                                          const float* __restrict__ phi_in,
-                                                          const float* __restrict__ rho,
-                                                          const float* __restrict__ sigma,
-                                                          const uint8_t* __restrict__ type,
-                                                          float* __restrict__ Hfine, float damping) {
+__device__ __forceinline__ void d_jacobi_coarse(int lx, int ly, int lz, float* __restrict__ phi_out,
+                                                const float* __restrict__ phi_in, const float* __restrict__ rho,
+                                                const float* __restrict__ sigma, const uint8_t* __restrict__ type,
+                                                float* __restrict__ Hfine, float damping, int64_t i) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int x = (int)(i % lx);
     const int64_t rem = i / lx;
@@ -191,6 +200,15 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_coarse(int lx, int ly, int lz
     result = clamp_f(result, 0.0f, 1e7f);
     if (isnan(result)) result = prev;
     phi_out[i] = result;
+}
+__global__ void __launch_bounds__(kBlock) k_jacobi_coarse(int lx, int ly, int lz, float* __restrict__ phi_out,
+                                                          const float* __restrict__ phi_in,
+                                                          const float* __restrict__ rho,
+                                                          const float* __restrict__ sigma,
+                                                          const uint8_t* __restrict__ type,
+                                                          float* __restrict__ Hfine, float damping) {
+    d_jacobi_coarse(lx, ly, lz, phi_out, phi_in, rho, sigma, type, Hfine, damping,
+                    (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- restriction
@@ -237,14 +255,14 @@ __device__ __forceinline__ float face_cond_sum(const float* __restrict__ sigma, 
 }
 
 // SH/mg_restrict.comp.glsl:118-195
-__global__ void __launch_bounds__(kBlock) k_restrict(int fx_, int fy_, int fz_, const float* __restrict__ phi_f,
+__device__ __forceinline__ void d_restrict(int fx_, int fy_, int fz_, const float* __restrict__ phi_f,
                                                      const float* __restrict__ rho_f,
                                                      const float* __restrict__ sig_f,
                                                      const uint8_t* __restrict__ type_f, int cx_, int cy_,
                                                      int cz_, float* __restrict__ phi_c,
-                                                     float* __restrict__ rho_c) {
+                                                     float* __restrict__ rho_c, int64_t gt_, int64_t blk_) {
     const int64_t nc = (int64_t)cx_ * cy_ * cz_;
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c = gt_;
     if (c >= nc) return;
     const int cx = (int)(c % cx_);
     const int64_t rem = c / cx_;
@@ -277,12 +295,20 @@ __global__ void __launch_bounds__(kBlock) k_restrict(int fx_, int fy_, int fz_, 
             }
     phi_c[c] = (tpw > 1e-20f) ? swp / tpw : (count > 0 ? sp / (float)count : 0.0f);
 }
+__global__ void __launch_bounds__(kBlock) k_restrict(int fx_, int fy_, int fz_, const float* __restrict__ phi_f,
+                                                     const float* __restrict__ rho_f,
+                                                     const float* __restrict__ sig_f,
+                                                     const uint8_t* __restrict__ type_f, int cx_, int cy_,
+                                                     int cz_, float* __restrict__ phi_c,
+                                                     float* __restrict__ rho_c) {
+    d_restrict(fx_, fy_, fz_, phi_f, rho_f, sig_f, type_f, cx_, cy_, cz_, phi_c, rho_c, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // SH/mg_prolong.comp.glsl:233-275 -- phi_f += trilinear(phi_c) at x/2
-__global__ void __launch_bounds__(kBlock) k_prolong(int fx_, int fy_, int fz_, float* __restrict__ phi_f, int cx_,
-                                                    int cy_, int cz_, const float* __restrict__ phi_c) {
+__device__ __forceinline__ void d_prolong(int fx_, int fy_, int fz_, float* __restrict__ phi_f, int cx_,
+                                                    int cy_, int cz_, const float* __restrict__ phi_c, int64_t gt_, int64_t blk_) {
     const int64_t nf = (int64_t)fx_ * fy_ * fz_;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     if (i >= nf) return;
     const int x = (int)(i % fx_);
     const int64_t rem = i / fx_;
@@ -308,16 +334,20 @@ __global__ void __launch_bounds__(kBlock) k_prolong(int fx_, int fy_, int fz_, f
 #undef MIXF
     phi_f[i] += corr;
 }
+__global__ void __launch_bounds__(kBlock) k_prolong(int fx_, int fy_, int fz_, float* __restrict__ phi_f, int cx_,
+                                                    int cy_, int cz_, const float* __restrict__ phi_c) {
+    d_prolong(fx_, fy_, fz_, phi_f, cx_, cy_, cz_, phi_c, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // island_buffer.cpp:600-700 (downsampleLevel), on the device: coarse
 // sigma_d = mean of the children, type = ANCHOR if any anchor child, SOLID
 // if solid children > contributing/2, else AIR.
-__global__ void __launch_bounds__(kBlock) k_downsample(int sx, int sy, int sz, const float* __restrict__ src_cond,
+__device__ __forceinline__ void d_downsample(int sx, int sy, int sz, const float* __restrict__ src_cond,
                                                        const uint8_t* __restrict__ src_type, int dx_, int dy_,
                                                        int dz_, float* __restrict__ out_cond,
-                                                       uint8_t* __restrict__ out_type) {
+                                                       uint8_t* __restrict__ out_type, int64_t gt_, int64_t blk_) {
     const int64_t dn = (int64_t)dx_ * dy_ * dz_;
-    const int64_t ci = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t ci = gt_;
     if (ci >= dn) return;
     const int cx = (int)(ci % dx_);
     const int64_t rem = ci / dx_;
@@ -341,6 +371,12 @@ __global__ void __launch_bounds__(kBlock) k_downsample(int sx, int sy, int sz, c
     for (int d = 0; d < 6; d++) out_cond[d * dn + ci] = contrib > 0 ? sum[d] * inv : 0.0f;
     out_type[ci] = anchor > 0 ? kAnchor : (solid > contrib / 2 ? kSolid : kAir);
 }
+__global__ void __launch_bounds__(kBlock) k_downsample(int sx, int sy, int sz, const float* __restrict__ src_cond,
+                                                       const uint8_t* __restrict__ src_type, int dx_, int dy_,
+                                                       int dz_, float* __restrict__ out_cond,
+                                                       uint8_t* __restrict__ out_type) {
+    d_downsample(sx, sy, sz, src_cond, src_type, dx_, dy_, dz_, out_cond, out_type, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // ---------------------------------------------------------------- PCG
 // 26-point diagonal with bounds-checked faces (pcg_update/pcg_direction computeDiag)
@@ -361,10 +397,10 @@ __device__ __forceinline__ float diag26_valid(const float s6[6], int x, int y, i
 }
 
 // SH/pcg_precompute.comp.glsl:24-86 (faces summed without a bounds check)
-__global__ void __launch_bounds__(kBlock) k_pcg_precompute(int lx, int ly, int lz, const float* __restrict__ sigma,
-                                                           float* __restrict__ invdiag) {
+__device__ __forceinline__ void d_pcg_precompute(int lx, int ly, int lz, const float* __restrict__ sigma,
+                                                           float* __restrict__ invdiag, int64_t gt_, int64_t blk_) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     if (i >= n) return;
     const int x = (int)(i % lx);
     const int64_t rem = i / lx;
@@ -382,6 +418,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg_precompute(int lx, int ly, int l
         d26 += corner_weight(s6, ci);
     }
     invdiag[i] = (d26 > 1e-20f) ? (1.0f / d26) : 0.0f;
+}
+__global__ void __launch_bounds__(kBlock) k_pcg_precompute(int lx, int ly, int lz, const float* __restrict__ sigma,
+                                                           float* __restrict__ invdiag) {
+    d_pcg_precompute(lx, ly, lz, sigma, invdiag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // Block-wide float sum (fixed shuffle tree, deterministic).  Result valid in thread 0.
@@ -404,12 +444,12 @@ __device__ __forceinline__ float block_sum(float v) {
 // SH/pcg_matvec.comp.glsl:128-214: out = sum_j w_ij (in_i - in_j); air/anchor rows 0.
 // If partial != nullptr, also emits per-block sums of in_i * out_i (pcg_dot pass 1
 // fused: the p.Ap product of pcg_dot.comp.glsl).
-__global__ void __launch_bounds__(kBlock) k_pcg_matvec(int lx, int ly, int lz, const float* __restrict__ in,
+__device__ __forceinline__ void d_pcg_matvec(int lx, int ly, int lz, const float* __restrict__ in,
                                                        float* __restrict__ out, const float* __restrict__ sigma,
                                                        const uint8_t* __restrict__ type,
-                                                       float* __restrict__ partial) {
+                                                       float* __restrict__ partial, int64_t gt_, int64_t blk_) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     float prod = 0.0f;
     if (i < n) {
         const int x = (int)(i % lx);
@@ -456,15 +496,21 @@ __global__ void __launch_bounds__(kBlock) k_pcg_matvec(int lx, int ly, int lz, c
     }
     if (partial != nullptr) {
         const float s = block_sum(prod);
-        if (threadIdx.x == 0) partial[blockIdx.x] = s;
+        if (threadIdx.x == 0) partial[blk_] = s;
     }
+}
+__global__ void __launch_bounds__(kBlock) k_pcg_matvec(int lx, int ly, int lz, const float* __restrict__ in,
+                                                       float* __restrict__ out, const float* __restrict__ sigma,
+                                                       const uint8_t* __restrict__ type,
+                                                       float* __restrict__ partial) {
+    d_pcg_matvec(lx, ly, lz, in, out, sigma, type, partial, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // SH/pcg_update.comp.glsl:116-211.  Init: r = s - Ap, z = r/diag, p = z.
 // Iteration: alpha = red[0]/red[1]; phi += alpha p (clamped), r = r_in - alpha Ap,
 // z = r/diag + (sum_d sigma_d r_in[j] invdiag[j]) / diag where r_in is r before
 // this dispatch.  Per-block partial of r.z over voxels i < rtz_limit.
-__global__ void __launch_bounds__(kBlock) k_pcg_update(int lx, int ly, int lz, float* __restrict__ phi,
+__device__ __forceinline__ void d_pcg_update(int lx, int ly, int lz, float* __restrict__ phi,
                                                        const float* __restrict__ r_in, float* __restrict__ r_out,
                                                        float* __restrict__ p, const float* __restrict__ ap,
                                                        const float* __restrict__ src,
@@ -472,9 +518,9 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(int lx, int ly, int lz, f
                                                        const float* __restrict__ sigma,
                                                        const float* __restrict__ invdiag,
                                                        const float* __restrict__ red, int is_init,
-                                                       int64_t rtz_limit, float* __restrict__ partial) {
+                                                       int64_t rtz_limit, float* __restrict__ partial, int64_t gt_, int64_t blk_) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     float rz = 0.0f;
     if (i < n) {
         const int x = (int)(i % lx);
@@ -526,16 +572,27 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(int lx, int ly, int lz, f
         if (i >= rtz_limit) rz = 0.0f;
     }
     const float s = block_sum(rz);
-    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    if (threadIdx.x == 0) partial[blk_] = s;
+}
+__global__ void __launch_bounds__(kBlock) k_pcg_update(int lx, int ly, int lz, float* __restrict__ phi,
+                                                       const float* __restrict__ r_in, float* __restrict__ r_out,
+                                                       float* __restrict__ p, const float* __restrict__ ap,
+                                                       const float* __restrict__ src,
+                                                       const uint8_t* __restrict__ type,
+                                                       const float* __restrict__ sigma,
+                                                       const float* __restrict__ invdiag,
+                                                       const float* __restrict__ red, int is_init,
+                                                       int64_t rtz_limit, float* __restrict__ partial) {
+    d_pcg_update(lx, ly, lz, phi, r_in, r_out, p, ap, src, type, sigma, invdiag, red, is_init, rtz_limit, partial, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // SH/pcg_direction.comp.glsl:336-379
-__global__ void __launch_bounds__(kBlock) k_pcg_direction(int lx, int ly, int lz, const float* __restrict__ r,
+__device__ __forceinline__ void d_pcg_direction(int lx, int ly, int lz, const float* __restrict__ r,
                                                           float* __restrict__ p, const uint8_t* __restrict__ type,
                                                           const float* __restrict__ red,
-                                                          const float* __restrict__ sigma) {
+                                                          const float* __restrict__ sigma, int64_t gt_, int64_t blk_) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     if (i >= n) return;
     if (type[i] != kSolid) { p[i] = 0.0f; return; }
     const int x = (int)(i % lx);
@@ -568,11 +625,17 @@ __global__ void __launch_bounds__(kBlock) k_pcg_direction(int lx, int ly, int lz
     if (!finite_f(np)) np = zi;
     p[i] = np;
 }
+__global__ void __launch_bounds__(kBlock) k_pcg_direction(int lx, int ly, int lz, const float* __restrict__ r,
+                                                          float* __restrict__ p, const uint8_t* __restrict__ type,
+                                                          const float* __restrict__ red,
+                                                          const float* __restrict__ sigma) {
+    d_pcg_direction(lx, ly, lz, r, p, type, red, sigma, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // Single-block sum of `count` partials into red[slot].  rotate: first copy
 // red[2] -> red[0] (the rTz slot rotation of dispatcher_pcg.cpp recordReductionRotate).
-__global__ void __launch_bounds__(kBlock) k_finalize(const float* __restrict__ partial, int64_t count,
-                                                     float* __restrict__ red, int slot, int rotate) {
+__device__ __forceinline__ void d_finalize(const float* __restrict__ partial, int64_t count,
+                                                     float* __restrict__ red, int slot, int rotate, int64_t gt_, int64_t blk_) {
     float v = 0.0f;
     for (int64_t k = threadIdx.x; k < count; k += kBlock) v += partial[k];
     const float s = block_sum(v);
@@ -581,20 +644,24 @@ __global__ void __launch_bounds__(kBlock) k_finalize(const float* __restrict__ p
         red[slot] = s;
     }
 }
+__global__ void __launch_bounds__(kBlock) k_finalize(const float* __restrict__ partial, int64_t count,
+                                                     float* __restrict__ red, int slot, int rotate) {
+    d_finalize(partial, count, red, slot, rotate, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // ---------------------------------------------------------------- phase field
 // SH/phase_field_evolve.comp.glsl:246-364.  The shader rewrites dField in place
 // while neighbours read it (a race); here every d_j comes from Dold, a copy of
 // the field taken before the pass.
-__global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, const float* __restrict__ phi,
+__device__ __forceinline__ void d_phase_field(int lx, int ly, int lz, const float* __restrict__ phi,
                                                         const float* __restrict__ H, float* __restrict__ D,
                                                         const float* __restrict__ Dold,
                                                         const float* __restrict__ sigma,
                                                         const uint8_t* __restrict__ type,
                                                         uint8_t* __restrict__ fail, const float* __restrict__ hyd,
-                                                        float l0, float gc, float relax, int split) {
+                                                        float l0, float gc, float relax, int split, int64_t gt_, int64_t blk_) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     if (i >= n) return;
     const uint8_t tp = type[i];
     if (tp == kAir || tp == kAnchor) return;
@@ -634,19 +701,28 @@ __global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, 
     D[i] = dn;
     if (dn > 0.95f) fail[i] = 1;
 }
+__global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, const float* __restrict__ phi,
+                                                        const float* __restrict__ H, float* __restrict__ D,
+                                                        const float* __restrict__ Dold,
+                                                        const float* __restrict__ sigma,
+                                                        const uint8_t* __restrict__ type,
+                                                        uint8_t* __restrict__ fail, const float* __restrict__ hyd,
+                                                        float l0, float gc, float relax, int split) {
+    d_phase_field(lx, ly, lz, phi, H, D, Dold, sigma, type, fail, hyd, l0, gc, relax, split, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // ---------------------------------------------------------------- failure scan
 // SH/failure_scan.comp.glsl:36-196
-__global__ void __launch_bounds__(kBlock) k_failure_scan(int lx, int ly, int lz, const float* __restrict__ phi,
+__device__ __forceinline__ void d_failure_scan(int lx, int ly, int lz, const float* __restrict__ phi,
                                                          const float* __restrict__ sigma,
                                                          const float* __restrict__ rcomp,
                                                          const uint8_t* __restrict__ type,
                                                          uint8_t* __restrict__ fail,
                                                          const float* __restrict__ rtens,
                                                          uint32_t* __restrict__ macro,
-                                                         const float* __restrict__ rho, float phi_orphan) {
+                                                         const float* __restrict__ rho, float phi_orphan, int64_t gt_, int64_t blk_) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = gt_;
     if (i >= n) return;
     uint8_t code = 0;
     if (type[i] != kSolid) { fail[i] = 0; return; }
@@ -705,16 +781,29 @@ __global__ void __launch_bounds__(kBlock) k_failure_scan(int lx, int ly, int lz,
     const int64_t mb = (x / kMacroBlock) + (int64_t)mbx * ((y / kMacroBlock) + (int64_t)mby * (z / kMacroBlock));
     atomicMax(macro + mb, __float_as_uint(res));
 }
+__global__ void __launch_bounds__(kBlock) k_failure_scan(int lx, int ly, int lz, const float* __restrict__ phi,
+                                                         const float* __restrict__ sigma,
+                                                         const float* __restrict__ rcomp,
+                                                         const uint8_t* __restrict__ type,
+                                                         uint8_t* __restrict__ fail,
+                                                         const float* __restrict__ rtens,
+                                                         uint32_t* __restrict__ macro,
+                                                         const float* __restrict__ rho, float phi_orphan) {
+    d_failure_scan(lx, ly, lz, phi, sigma, rcomp, type, fail, rtens, macro, rho, phi_orphan, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
-__global__ void k_macro_fill(uint32_t* __restrict__ macro, int64_t nmb) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void d_macro_fill(uint32_t* __restrict__ macro, int64_t nmb, int64_t gt_, int64_t blk_) {
+    const int64_t i = gt_;
     if (i < nmb) macro[i] = kMacroSeedBits;
+}
+__global__ void k_macro_fill(uint32_t* __restrict__ macro, int64_t nmb) {
+    d_macro_fill(macro, nmb, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // max over macro blocks as float (readbackMacroResidualMax, island_buffer.cpp:1012-1090),
 // single block; writes out[0].
-__global__ void __launch_bounds__(kBlock) k_macro_max(const uint32_t* __restrict__ macro, int64_t nmb,
-                                                      float* __restrict__ out) {
+__device__ __forceinline__ void d_macro_max(const uint32_t* __restrict__ macro, int64_t nmb,
+                                                      float* __restrict__ out, int64_t gt_, int64_t blk_) {
     __shared__ float warp_part[kBlock / 32];
     float m = 0.0f;
     for (int64_t k = threadIdx.x; k < nmb; k += kBlock) m = fmaxf(m, __uint_as_float(macro[k]));
@@ -729,26 +818,34 @@ __global__ void __launch_bounds__(kBlock) k_macro_max(const uint32_t* __restrict
         if (threadIdx.x == 0) out[0] = s;
     }
 }
+__global__ void __launch_bounds__(kBlock) k_macro_max(const uint32_t* __restrict__ macro, int64_t nmb,
+                                                      float* __restrict__ out) {
+    d_macro_max(macro, nmb, out, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // ---------------------------------------------------------------- failure compaction
 constexpr int kCompactChunk = 4096;  // voxels per block
 
-__global__ void __launch_bounds__(kBlock) k_fail_count(const uint8_t* __restrict__ fail, int64_t n,
-                                                       int32_t* __restrict__ counts) {
-    const int64_t base = (int64_t)blockIdx.x * kCompactChunk;
+__device__ __forceinline__ void d_fail_count(const uint8_t* __restrict__ fail, int64_t n,
+                                                       int32_t* __restrict__ counts, int64_t gt_, int64_t blk_) {
+    const int64_t base = (int64_t)blk_ * kCompactChunk;
     int c = 0;
     for (int k = threadIdx.x; k < kCompactChunk; k += kBlock) {
         const int64_t i = base + k;
         if (i < n && fail[i] != 0) c++;
     }
     const float s = block_sum((float)c);
-    if (threadIdx.x == 0) counts[blockIdx.x] = (int32_t)s;
+    if (threadIdx.x == 0) counts[blk_] = (int32_t)s;
+}
+__global__ void __launch_bounds__(kBlock) k_fail_count(const uint8_t* __restrict__ fail, int64_t n,
+                                                       int32_t* __restrict__ counts) {
+    d_fail_count(fail, n, counts, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // exclusive scan of block counts (single block, sequential over chunks of 256);
 // writes offsets[] and total[0].
-__global__ void __launch_bounds__(kBlock) k_fail_scan(const int32_t* __restrict__ counts, int64_t nblocks,
-                                                      int32_t* __restrict__ offsets, int32_t* __restrict__ total) {
+__device__ __forceinline__ void d_fail_scan(const int32_t* __restrict__ counts, int64_t nblocks,
+                                                      int32_t* __restrict__ offsets, int32_t* __restrict__ total, int64_t gt_, int64_t blk_) {
     __shared__ int32_t buf[kBlock];
     __shared__ int32_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -771,17 +868,21 @@ __global__ void __launch_bounds__(kBlock) k_fail_scan(const int32_t* __restrict_
     }
     if (threadIdx.x == 0) total[0] = carry;
 }
+__global__ void __launch_bounds__(kBlock) k_fail_scan(const int32_t* __restrict__ counts, int64_t nblocks,
+                                                      int32_t* __restrict__ offsets, int32_t* __restrict__ total) {
+    d_fail_scan(counts, nblocks, offsets, total, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // write {x+ox, y+oy, z+oz, code} tuples in index order; tuples beyond cap are dropped.
-__global__ void __launch_bounds__(kBlock) k_fail_write(const uint8_t* __restrict__ fail, int lx, int ly, int lz,
+__device__ __forceinline__ void d_fail_write(const uint8_t* __restrict__ fail, int lx, int ly, int lz,
                                                        int ox, int oy, int oz,
                                                        const int32_t* __restrict__ offsets,
-                                                       int32_t* __restrict__ tuples, int32_t cap) {
+                                                       int32_t* __restrict__ tuples, int32_t cap, int64_t gt_, int64_t blk_) {
     __shared__ int32_t warp_cnt[kBlock / 32];
     __shared__ int32_t run;
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t base = (int64_t)blockIdx.x * kCompactChunk;
-    if (threadIdx.x == 0) run = offsets[blockIdx.x];
+    const int64_t base = (int64_t)blk_ * kCompactChunk;
+    if (threadIdx.x == 0) run = offsets[blk_];
     __syncthreads();
     for (int k0 = 0; k0 < kCompactChunk; k0 += kBlock) {
         const int64_t i = base + k0 + threadIdx.x;
@@ -809,6 +910,12 @@ __global__ void __launch_bounds__(kBlock) k_fail_write(const uint8_t* __restrict
         __syncthreads();
     }
 }
+__global__ void __launch_bounds__(kBlock) k_fail_write(const uint8_t* __restrict__ fail, int lx, int ly, int lz,
+                                                       int ox, int oy, int oz,
+                                                       const int32_t* __restrict__ offsets,
+                                                       int32_t* __restrict__ tuples, int32_t cap) {
+    d_fail_write(fail, lx, ly, lz, ox, oy, oz, offsets, tuples, cap, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
+}
 
 // SH/sparse_scatter.comp.glsl: 48-byte records {u32 idx, f32 source, u32 type,
 // f32 maxPhi, f32 rcomp, f32 rtens, f32 cond[6]} scattered into the SoA arrays.
@@ -830,6 +937,181 @@ __global__ void k_sparse_scatter(const uint32_t* __restrict__ rec, int count, in
 #pragma unroll
     for (int d = 0; d < 6; d++) cond[d * n + i] = __uint_as_float(r[6 + d]);
 }
+
+// ---------------------------------------------------------------- batched forms
+using compat::CIsl;
+// Block b of a batched launch belongs to the island q whose block range
+// [bs[q], bs[q+1]) holds it (islands with no blocks of this kind are
+// skipped by the search); found once per block by thread 0.
+__device__ __forceinline__ int b_island(const int* __restrict__ bs, int nisl) {
+    __shared__ int s_q;
+    if (threadIdx.x == 0) {
+        const int b = (int)blockIdx.x;
+        int lo = 0, hi = nisl - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bs[mid] <= b) lo = mid;
+            else hi = mid - 1;
+        }
+        s_q = lo;
+    }
+    __syncthreads();
+    return s_q;
+}
+
+#define BATCH_ISLAND                                                   \
+    const int q_ = b_island(bs, nisl);                                 \
+    const CIsl& I = tab[q_];                                           \
+    const int64_t lb_ = (int64_t)blockIdx.x - (int64_t)bs[q_];         \
+    const int64_t t_ = lb_ * (int64_t)blockDim.x + threadIdx.x;
+
+__device__ __forceinline__ float b_damping(const CIsl& I, int sidx, int warm, float dampf) {
+    return I.iter0 + sidx >= warm ? dampf : 0.0f;
+}
+
+// The caller's arrays into the device arrays (uploadFromHosts), read through
+// the device-visible mappings of the pinned host buffers.
+__global__ void __launch_bounds__(kBlock) kb_upload(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                    int nisl) {
+    BATCH_ISLAND
+    if (t_ >= I.n || I.h_phi == nullptr) return;
+    const int64_t i = t_, n = I.n;
+    I.phi[i] = I.h_phi[i];
+    I.src[i] = I.h_src[i];
+#pragma unroll
+    for (int d = 0; d < 6; d++) I.sigma[d * n + i] = I.h_sigma[d * n + i];
+    I.type[i] = I.h_type[i];
+    I.rcomp[i] = I.h_rcomp[i];
+    I.rtens[i] = I.h_rtens[i];
+    I.maxphi[i] = I.h_maxphi[i];
+    if (I.h_curing) I.hyd[i] = I.h_curing[i];
+}
+__global__ void __launch_bounds__(kBlock) kb_macro_fill(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl) {
+    BATCH_ISLAND
+    d_macro_fill(I.macro, I.nmb, t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_rbgs_color(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl, int color, int sidx, int warm, float dampf) {
+    BATCH_ISLAND
+    d_rbgs_color(I.lx, I.ly, I.lz, I.phi, I.src, I.sigma, I.type, I.H, I.macro, color,
+                 b_damping(I, sidx, warm, dampf), t_);
+}
+__global__ void __launch_bounds__(kBlock) kb_jacobi(const CIsl* __restrict__ tab, const int* __restrict__ bs, int nisl,
+                                                    int level, int flip, int sidx, int warm, float dampf) {
+    BATCH_ISLAND
+    const float damping = b_damping(I, sidx, warm, dampf);
+    if (level == 1) {
+        const int c = (I.cur1 + flip) & 1;
+        d_jacobi_coarse(I.l1x, I.l1y, I.l1z, I.phi1[1 - c], I.phi1[c], I.src1, I.sig1, I.type1, I.H, damping, t_);
+    } else {
+        const int c = (I.cur2 + flip) & 1;
+        d_jacobi_coarse(I.l2x, I.l2y, I.l2z, I.phi2[1 - c], I.phi2[c], I.src2, I.sig2, I.type2, I.H, damping, t_);
+    }
+}
+__global__ void __launch_bounds__(kBlock) kb_restrict(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                      int nisl, int level, int f1, int f2) {
+    BATCH_ISLAND
+    const int c1 = (I.cur1 + f1) & 1, c2 = (I.cur2 + f2) & 1;
+    if (level == 1)
+        d_restrict(I.lx, I.ly, I.lz, I.phi, I.src, I.sigma, I.type, I.l1x, I.l1y, I.l1z, I.phi1[c1], I.src1, t_, lb_);
+    else
+        d_restrict(I.l1x, I.l1y, I.l1z, I.phi1[c1], I.src1, I.sig1, I.type1, I.l2x, I.l2y, I.l2z, I.phi2[c2], I.src2,
+                   t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_prolong(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                     int nisl, int level, int f1, int f2) {
+    BATCH_ISLAND
+    const int c1 = (I.cur1 + f1) & 1, c2 = (I.cur2 + f2) & 1;
+    if (level == 1) d_prolong(I.lx, I.ly, I.lz, I.phi, I.l1x, I.l1y, I.l1z, I.phi1[c1], t_, lb_);
+    else d_prolong(I.l1x, I.l1y, I.l1z, I.phi1[c1], I.l2x, I.l2y, I.l2z, I.phi2[c2], t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_downsample(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl, int level) {
+    BATCH_ISLAND
+    if (level == 1) d_downsample(I.lx, I.ly, I.lz, I.sigma, I.type, I.l1x, I.l1y, I.l1z, I.sig1, I.type1, t_, lb_);
+    else d_downsample(I.l1x, I.l1y, I.l1z, I.sig1, I.type1, I.l2x, I.l2y, I.l2z, I.sig2, I.type2, t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_pcg_precompute(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                            int nisl) {
+    BATCH_ISLAND
+    d_pcg_precompute(I.lx, I.ly, I.lz, I.sigma, I.invdiag, t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_pcg_matvec(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl, int which) {
+    BATCH_ISLAND
+    if (which == 0) d_pcg_matvec(I.lx, I.ly, I.lz, I.phi, I.ap, I.sigma, I.type, nullptr, t_, lb_);
+    else d_pcg_matvec(I.lx, I.ly, I.lz, I.p, I.ap, I.sigma, I.type, I.partial, t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_pcg_update(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl, int is_init, int fr) {
+    BATCH_ISLAND
+    const int c = (I.rcur + fr) & 1;
+    const int64_t g = (I.n + 511) / 512;
+    const int64_t rtz = I.n < 256 * g ? I.n : 256 * g;
+    d_pcg_update(I.lx, I.ly, I.lz, I.phi, I.r[c], is_init ? I.r[c] : I.r[1 - c], I.p, I.ap, I.src, I.type, I.sigma,
+                 I.invdiag, I.red, is_init, rtz, I.partial, t_, lb_);
+}
+// one block per island
+__global__ void __launch_bounds__(kBlock) kb_finalize(const CIsl* __restrict__ tab, int slot, int rotate) {
+    const CIsl& I = tab[blockIdx.x];
+    d_finalize(I.partial, ceil_div64(I.n, kBlock), I.red, slot, rotate, 0, 0);
+}
+__global__ void __launch_bounds__(kBlock) kb_pcg_direction(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                           int nisl, int fr) {
+    BATCH_ISLAND
+    d_pcg_direction(I.lx, I.ly, I.lz, I.r[(I.rcur + fr) & 1], I.p, I.type, I.red, I.sigma, t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_copy_damage(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                         int nisl) {
+    BATCH_ISLAND
+    if (t_ < I.n) I.Dold[t_] = I.D[t_];
+}
+__global__ void __launch_bounds__(kBlock) kb_phase_field(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                         int nisl, float l0, float gc, float relax, int split) {
+    BATCH_ISLAND
+    d_phase_field(I.lx, I.ly, I.lz, I.phi, I.H, I.D, I.Dold, I.sigma, I.type, I.fail, I.hyd, l0, gc, relax, split,
+                  t_, lb_);
+}
+__global__ void __launch_bounds__(kBlock) kb_history(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                     int nisl) {
+    BATCH_ISLAND
+    d_history(I.lx, I.ly, I.lz, I.phi, I.sigma, I.type, I.H, t_);
+}
+__global__ void __launch_bounds__(kBlock) kb_failure_scan(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                          int nisl) {
+    BATCH_ISLAND
+    d_failure_scan(I.lx, I.ly, I.lz, I.phi, I.sigma, I.rcomp, I.type, I.fail, I.rtens, I.macro, I.src, kPhiOrphan,
+                   t_, lb_);
+}
+// one block per island
+__global__ void __launch_bounds__(kBlock) kb_macro_max(const CIsl* __restrict__ tab) {
+    const CIsl& I = tab[blockIdx.x];
+    d_macro_max(I.macro, I.nmb, I.res_macro, 0, 0);
+}
+__global__ void __launch_bounds__(kBlock) kb_fail_count(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl) {
+    BATCH_ISLAND
+    d_fail_count(I.fail, I.n, I.fcounts, t_, lb_);
+}
+// one block per island
+__global__ void __launch_bounds__(kBlock) kb_fail_scan(const CIsl* __restrict__ tab) {
+    const CIsl& I = tab[blockIdx.x];
+    d_fail_scan(I.fcounts, ceil_div64(I.n, kCompactChunk), I.foffsets, I.res_fail, 0, 0);
+}
+__global__ void __launch_bounds__(kBlock) kb_fail_write(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl) {
+    BATCH_ISLAND
+    d_fail_write(I.fail, I.lx, I.ly, I.lz, I.ox, I.oy, I.oz, I.foffsets, I.tuples, I.tuples ? I.tuple_cap : 0, t_,
+                 lb_);
+}
+// phi into the caller's stress readback buffer (device-visible host memory)
+__global__ void __launch_bounds__(kBlock) kb_stress_out(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl) {
+    BATCH_ISLAND
+    if (I.h_stress && t_ < I.stress_n) I.h_stress[t_] = I.phi[t_];
+}
+#undef BATCH_ISLAND
 
 inline unsigned grid_for(int64_t n) { return (unsigned)ceil_div64(n, kBlock); }
 
@@ -918,6 +1200,71 @@ void fail_compact(cudaStream_t s, const uint8_t* fail, int lx, int ly, int lz, i
     k_fail_scan<<<1, kBlock, 0, s>>>(counts, nb, offsets, total);
     k_fail_write<<<(unsigned)nb, kBlock, 0, s>>>(fail, lx, ly, lz, ox, oy, oz, offsets, tuples, cap);
 }
+
+int64_t batch_blocks(const CIsl& I, int kind) {
+    if (kind == kbN) return ceil_div64(I.n, kBlock);
+    if (kind >= kbC0 && kind < kbC0 + 8) {
+        const int c = kind - kbC0;
+        const int cx = c & 1, cy = (c >> 1) & 1, cz = (c >> 2) & 1;
+        const int64_t nc = (int64_t)((I.lx - cx + 1) >> 1) * ((I.ly - cy + 1) >> 1) * ((I.lz - cz + 1) >> 1);
+        return nc > 0 ? ceil_div64(nc, kBlock) : 0;
+    }
+    if (kind == kbN1) return ceil_div64(I.n1, kBlock);
+    if (kind == kbN2) return ceil_div64(I.n2, kBlock);
+    if (kind == kbMB) return ceil_div64(I.nmb, kBlock);
+    if (kind == kbFC) return ceil_div64(I.n, kCompactChunk);
+    return 0;
+}
+
+namespace batch {
+namespace {
+inline const int* row(const BGroup& g, int kind) { return g.bstart + (int64_t)kind * (g.nisl + 1); }
+}  // namespace
+#define BLAUNCH(kind, kern, ...)                                                                         \
+    do {                                                                                                 \
+        if (g.nisl > 0 && g.blocks[kind] > 0)                                                           \
+            kern<<<(unsigned)g.blocks[kind], kBlock, 0, s>>>(g.tab, row(g, kind), g.nisl, ##__VA_ARGS__); \
+    } while (0)
+
+void upload(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_upload); }
+void macro_fill(cudaStream_t s, const BGroup& g) { BLAUNCH(kbMB, kb_macro_fill); }
+void rbgs_color(cudaStream_t s, const BGroup& g, int color, int sidx, int warm, float dampf) {
+    BLAUNCH(kbC0 + color, kb_rbgs_color, color, sidx, warm, dampf);
+}
+void jacobi(cudaStream_t s, const BGroup& g, int level, int flip, int sidx, int warm, float dampf) {
+    BLAUNCH(level == 1 ? kbN1 : kbN2, kb_jacobi, level, flip, sidx, warm, dampf);
+}
+void restrict_to(cudaStream_t s, const BGroup& g, int level, int f1, int f2) {
+    BLAUNCH(level == 1 ? kbN1 : kbN2, kb_restrict, level, f1, f2);
+}
+void prolong_from(cudaStream_t s, const BGroup& g, int level, int f1, int f2) {
+    BLAUNCH(level == 1 ? kbN : kbN1, kb_prolong, level, f1, f2);
+}
+void downsample(cudaStream_t s, const BGroup& g, int level) { BLAUNCH(level == 1 ? kbN1 : kbN2, kb_downsample, level); }
+void pcg_precompute(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_pcg_precompute); }
+void pcg_matvec(cudaStream_t s, const BGroup& g, int which) { BLAUNCH(kbN, kb_pcg_matvec, which); }
+void pcg_update(cudaStream_t s, const BGroup& g, int is_init, int fr) { BLAUNCH(kbN, kb_pcg_update, is_init, fr); }
+void finalize(cudaStream_t s, const BGroup& g, int slot, int rotate) {
+    if (g.nisl > 0) kb_finalize<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab, slot, rotate);
+}
+void pcg_direction(cudaStream_t s, const BGroup& g, int fr) { BLAUNCH(kbN, kb_pcg_direction, fr); }
+void copy_damage(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_copy_damage); }
+void phase_field(cudaStream_t s, const BGroup& g, float l0, float gc, float relax, int split) {
+    BLAUNCH(kbN, kb_phase_field, l0, gc, relax, split);
+}
+void history(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_history); }
+void failure_scan(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_failure_scan); }
+void macro_max(cudaStream_t s, const BGroup& g) {
+    if (g.nisl > 0) kb_macro_max<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab);
+}
+void fail_compact(cudaStream_t s, const BGroup& g) {
+    BLAUNCH(kbFC, kb_fail_count);
+    if (g.nisl > 0) kb_fail_scan<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab);
+    BLAUNCH(kbFC, kb_fail_write);
+}
+void stress_out(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_stress_out); }
+#undef BLAUNCH
+}  // namespace batch
 
 void sparse_scatter(cudaStream_t s, const void* records, int count, int64_t n, float* source, float* cond,
                     uint8_t* type, float* maxphi, float* rcomp, float* rtens) {

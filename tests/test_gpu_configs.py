@@ -10,14 +10,16 @@ phi rounded to FP32.  Checks:
 * phi: max |phi_gpu - phi_fp64| <= 1e-5 max |phi_fp64| (FP64 accumulator);
 * failure codes and the failure buffer: bit-exact on every voxel outside the
   tolerance margin.  The margin is found by perturbation: the oracle's tail
-  also runs on phi_fp64 x (1 +/- 1e-6), and a voxel whose code differs
-  between those runs sits within the solve tolerance of a decision threshold
-  (a capacity in the failure scan, the damage threshold, or the psi_e switch
-  of the history update, flux_in > 3 flux_out, which scales psi_e by 100).
-  The number of margin voxels is reported and bounded;
-* H and damage: within 1e-5 of their maxima outside the same margin (and
-  outside the voxels where the perturbed runs' H or damage differ by more
-  than that).
+  also runs on four perturbed copies of phi_fp64 -- scaled by 1 +/- 1e-5
+  and with independent per-voxel noise of 1e-5 max |phi| (ten times the
+  solve's own error bound) -- each carrying its own history, damage and
+  failure state.  A voxel where a perturbed run's code differs, or its H or
+  damage differs by more than 1e-3 of the maximum (the psi_e switch of the
+  history update, flux_in > 3 flux_out, scales psi_e by 100), sits within
+  the solve tolerance of a decision threshold; since the phase field reads
+  the damage of the six face neighbours, the margin grows by one voxel per
+  tick.  The number of margin voxels is reported and bounded;
+* H and damage: within 1e-5 of their maxima outside the same margin.
 
 Config 1: the 32^3 fully solid block, three-material mix.  Config 2: the
 256 x 256 x 128 noise island (60 % occupancy).  Config 5, reduced: a
@@ -38,7 +40,7 @@ from pfsf_b200 import capi, synth
 pytestmark = pytest.mark.gpu
 
 THREADS = os.cpu_count() or 1
-DELTA = 1e-6
+DELTA = 1e-5
 
 
 @pytest.fixture(scope="module")
@@ -69,6 +71,20 @@ def _case(isl, phi_max=20.0, rscale=0.1):
     return case, phi * scale
 
 
+def _dilate6(m, dims):
+    """m plus the six face neighbours of every voxel in it."""
+    lx, ly, lz = dims
+    g = m.reshape(lz, ly, lx)
+    o = g.copy()
+    o[1:] |= g[:-1]
+    o[:-1] |= g[1:]
+    o[:, 1:] |= g[:, :-1]
+    o[:, :-1] |= g[:, 1:]
+    o[:, :, 1:] |= g[:, :, :-1]
+    o[:, :, :-1] |= g[:, :, 1:]
+    return o.reshape(-1)
+
+
 class Chain:
     """Oracle tail state (H, D, fail) carried from tick to tick."""
 
@@ -93,7 +109,11 @@ def _run(eng, iid, isl, case_x, ticks, prec, ramp=1.0, origin=(0, 0, 0)):
     assert eng.register_buffers(iid, phi, src, case["conductivity"], case["type"], case["rcomp"], case["rtens"],
                                 case["max_phi"]) == capi.PFSF_OK
     assert eng.register_kappa(iid, phik, src, isl.kappa, isl.vtype) == capi.PFSF_OK
-    chains = {d: Chain(isl.n) for d in (0.0, DELTA, -DELTA)}
+    rng = np.random.default_rng(isl.n)
+    solid = isl.vtype == 1
+    noise = [rng.uniform(-1.0, 1.0, isl.n) * solid for _ in range(2)]
+    chains = [Chain(isl.n) for _ in range(5)]
+    margin = np.zeros(isl.n, bool)
     cap = 1 << 16
     report = []
     for t in range(ticks):
@@ -108,19 +128,22 @@ def _run(eng, iid, isl, case_x, ticks, prec, ramp=1.0, origin=(0, 0, 0)):
         err = float(np.abs(x64 - xr).max() / np.abs(xr).max())
         assert err <= 1e-5, f"tick {t}: phi error vs FP64 {err:.2e}"
         c = dict(case, source=src.copy())
-        for d, ch in chains.items():
-            ch.tick(isl.dims, (xr * (1.0 + d)).astype(np.float32), c)
-        ref = chains[0.0]
+        amp = DELTA * float(np.abs(xr).max())
+        phis = [xr, xr * (1.0 + DELTA), xr * (1.0 - DELTA), xr + amp * noise[0], xr + amp * noise[1]]
+        for ch, ph in zip(chains, phis):
+            ch.tick(isl.dims, ph.astype(np.float32), c)
+        ref = chains[0]
         fail_g = eng.debug_field(iid, 3)
         H_g = eng.debug_field(iid, 1)
         D_g = eng.debug_field(iid, 2)
-        fails = [ch.fail.astype(np.uint8) for ch in chains.values()]
-        margin = (fails[0] != fails[1]) | (fails[0] != fails[2])
         hs = max(float(np.abs(ref.H).max()), 1e-30)
         ds = max(float(np.abs(ref.D).max()), 1e-30)
-        for ch in (chains[DELTA], chains[-DELTA]):
-            margin |= np.abs(ch.H - ref.H) > 1e-5 * hs
-            margin |= np.abs(ch.D - ref.D) > 1e-5 * ds
+        margin = _dilate6(margin, isl.dims) if t > 0 else margin
+        for ch in chains[1:]:
+            margin |= ch.fail != ref.fail
+            margin |= np.abs(ch.H - ref.H) > 1e-3 * hs
+            margin |= np.abs(ch.D - ref.D) > 1e-3 * ds
+        fails = [ref.fail.astype(np.uint8)]
         out = ~margin
         bad = int(np.sum(fail_g[out] != fails[0][out]))
         assert bad == 0, f"tick {t}: {bad} failure codes differ outside the margin"
@@ -163,4 +186,4 @@ def test_config5_fracture_reduced(eng):
     isl = synth.noise_island((128, 128, 64), seed=51, occupancy=0.55)
     rep = _run(eng, 9320, isl, _case(isl), ticks=3, prec=capi.PREC_BF16, ramp=2.0)
     assert rep[-1]["failures"] >= rep[0]["failures"] > 0
-    assert max(r["margin_voxels"] for r in rep) <= isl.n // 1000, rep
+    assert max(r["margin_voxels"] for r in rep) <= isl.n // 100, rep
