@@ -134,15 +134,6 @@ __device__ __forceinline__ void d_rbgs_color(int lx, int ly, int lz, float* __re
     if (isnan(result)) result = phi[i];
     phi[i] = result;
 }
-__global__ void __launch_bounds__(kBlock) k_rbgs_color(int lx, int ly, int lz, float* __restrict__ phi,
-                                                       const float* __restrict__ rho,
-                                                       const float* __restrict__ sigma,
-                                                       const uint8_t* __restrict__ type, float* __restrict__ H,
-                                                       const uint32_t* __restrict__ macro, int color,
-                                                       float damping) {
-    d_rbgs_color(lx, ly, lz, phi, rho, sigma, type, H, macro, color, damping,
-                 (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
-}
 
 
 // ---------------------------------------------------------------- history
@@ -166,11 +157,6 @@ __device__ __forceinline__ void d_history(int lx, int ly, int lz, const float* _
         nphi6[d] = inb(nx, ny, nz, lx, ly, lz) ? phi[gidx(nx, ny, nz, lx, ly)] : 0.0f;
     }
     H[i] = fmaxf(H[i], amor_psi(s6, nphi6, x, y, z, lx, ly, lz, p));
-}
-__global__ void __launch_bounds__(kBlock) k_history(int lx, int ly, int lz, const float* __restrict__ phi,
-                                                    const float* __restrict__ sigma,
-                                                    const uint8_t* __restrict__ type, float* __restrict__ H) {
-    d_history(lx, ly, lz, phi, sigma, type, H, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- coarse Jacobi
@@ -200,15 +186,6 @@ __device__ __forceinline__ void d_jacobi_coarse(int lx, int ly, int lz, float* _
     result = clamp_f(result, 0.0f, 1e7f);
     if (isnan(result)) result = prev;
     phi_out[i] = result;
-}
-__global__ void __launch_bounds__(kBlock) k_jacobi_coarse(int lx, int ly, int lz, float* __restrict__ phi_out,
-                                                          const float* __restrict__ phi_in,
-                                                          const float* __restrict__ rho,
-                                                          const float* __restrict__ sigma,
-                                                          const uint8_t* __restrict__ type,
-                                                          float* __restrict__ Hfine, float damping) {
-    d_jacobi_coarse(lx, ly, lz, phi_out, phi_in, rho, sigma, type, Hfine, damping,
-                    (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- restriction
@@ -295,14 +272,6 @@ __device__ __forceinline__ void d_restrict(int fx_, int fy_, int fz_, const floa
             }
     phi_c[c] = (tpw > 1e-20f) ? swp / tpw : (count > 0 ? sp / (float)count : 0.0f);
 }
-__global__ void __launch_bounds__(kBlock) k_restrict(int fx_, int fy_, int fz_, const float* __restrict__ phi_f,
-                                                     const float* __restrict__ rho_f,
-                                                     const float* __restrict__ sig_f,
-                                                     const uint8_t* __restrict__ type_f, int cx_, int cy_,
-                                                     int cz_, float* __restrict__ phi_c,
-                                                     float* __restrict__ rho_c) {
-    d_restrict(fx_, fy_, fz_, phi_f, rho_f, sig_f, type_f, cx_, cy_, cz_, phi_c, rho_c, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
-}
 
 // SH/mg_prolong.comp.glsl:233-275 -- phi_f += trilinear(phi_c) at x/2
 __device__ __forceinline__ void d_prolong(int fx_, int fy_, int fz_, float* __restrict__ phi_f, int cx_,
@@ -333,10 +302,6 @@ __device__ __forceinline__ void d_prolong(int fx_, int fy_, int fz_, float* __re
                             MIXF(MIXF(c[1][0][0], c[1][0][1], wx), MIXF(c[1][1][0], c[1][1][1], wx), wy), wz);
 #undef MIXF
     phi_f[i] += corr;
-}
-__global__ void __launch_bounds__(kBlock) k_prolong(int fx_, int fy_, int fz_, float* __restrict__ phi_f, int cx_,
-                                                    int cy_, int cz_, const float* __restrict__ phi_c) {
-    d_prolong(fx_, fy_, fz_, phi_f, cx_, cy_, cz_, phi_c, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // island_buffer.cpp:600-700 (downsampleLevel), on the device: coarse
@@ -370,12 +335,6 @@ __device__ __forceinline__ void d_downsample(int sx, int sy, int sz, const float
 #pragma unroll
     for (int d = 0; d < 6; d++) out_cond[d * dn + ci] = contrib > 0 ? sum[d] * inv : 0.0f;
     out_type[ci] = anchor > 0 ? kAnchor : (solid > contrib / 2 ? kSolid : kAir);
-}
-__global__ void __launch_bounds__(kBlock) k_downsample(int sx, int sy, int sz, const float* __restrict__ src_cond,
-                                                       const uint8_t* __restrict__ src_type, int dx_, int dy_,
-                                                       int dz_, float* __restrict__ out_cond,
-                                                       uint8_t* __restrict__ out_type) {
-    d_downsample(sx, sy, sz, src_cond, src_type, dx_, dy_, dz_, out_cond, out_type, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // ---------------------------------------------------------------- PCG
@@ -418,10 +377,6 @@ __device__ __forceinline__ void d_pcg_precompute(int lx, int ly, int lz, const f
         d26 += corner_weight(s6, ci);
     }
     invdiag[i] = (d26 > 1e-20f) ? (1.0f / d26) : 0.0f;
-}
-__global__ void __launch_bounds__(kBlock) k_pcg_precompute(int lx, int ly, int lz, const float* __restrict__ sigma,
-                                                           float* __restrict__ invdiag) {
-    d_pcg_precompute(lx, ly, lz, sigma, invdiag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // Block-wide float sum (fixed shuffle tree, deterministic).  Result valid in thread 0.
@@ -499,12 +454,6 @@ __device__ __forceinline__ void d_pcg_matvec(int lx, int ly, int lz, const float
         if (threadIdx.x == 0) partial[blk_] = s;
     }
 }
-__global__ void __launch_bounds__(kBlock) k_pcg_matvec(int lx, int ly, int lz, const float* __restrict__ in,
-                                                       float* __restrict__ out, const float* __restrict__ sigma,
-                                                       const uint8_t* __restrict__ type,
-                                                       float* __restrict__ partial) {
-    d_pcg_matvec(lx, ly, lz, in, out, sigma, type, partial, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
-}
 
 // SH/pcg_update.comp.glsl:116-211.  Init: r = s - Ap, z = r/diag, p = z.
 // Iteration: alpha = red[0]/red[1]; phi += alpha p (clamped), r = r_in - alpha Ap,
@@ -574,17 +523,6 @@ __device__ __forceinline__ void d_pcg_update(int lx, int ly, int lz, float* __re
     const float s = block_sum(rz);
     if (threadIdx.x == 0) partial[blk_] = s;
 }
-__global__ void __launch_bounds__(kBlock) k_pcg_update(int lx, int ly, int lz, float* __restrict__ phi,
-                                                       const float* __restrict__ r_in, float* __restrict__ r_out,
-                                                       float* __restrict__ p, const float* __restrict__ ap,
-                                                       const float* __restrict__ src,
-                                                       const uint8_t* __restrict__ type,
-                                                       const float* __restrict__ sigma,
-                                                       const float* __restrict__ invdiag,
-                                                       const float* __restrict__ red, int is_init,
-                                                       int64_t rtz_limit, float* __restrict__ partial) {
-    d_pcg_update(lx, ly, lz, phi, r_in, r_out, p, ap, src, type, sigma, invdiag, red, is_init, rtz_limit, partial, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
-}
 
 // SH/pcg_direction.comp.glsl:336-379
 __device__ __forceinline__ void d_pcg_direction(int lx, int ly, int lz, const float* __restrict__ r,
@@ -625,12 +563,6 @@ __device__ __forceinline__ void d_pcg_direction(int lx, int ly, int lz, const fl
     if (!finite_f(np)) np = zi;
     p[i] = np;
 }
-__global__ void __launch_bounds__(kBlock) k_pcg_direction(int lx, int ly, int lz, const float* __restrict__ r,
-                                                          float* __restrict__ p, const uint8_t* __restrict__ type,
-                                                          const float* __restrict__ red,
-                                                          const float* __restrict__ sigma) {
-    d_pcg_direction(lx, ly, lz, r, p, type, red, sigma, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
-}
 
 // Single-block sum of `count` partials into red[slot].  rotate: first copy
 // red[2] -> red[0] (the rTz slot rotation of dispatcher_pcg.cpp recordReductionRotate).
@@ -643,10 +575,6 @@ __device__ __forceinline__ void d_finalize(const float* __restrict__ partial, in
         if (rotate) red[0] = red[2];
         red[slot] = s;
     }
-}
-__global__ void __launch_bounds__(kBlock) k_finalize(const float* __restrict__ partial, int64_t count,
-                                                     float* __restrict__ red, int slot, int rotate) {
-    d_finalize(partial, count, red, slot, rotate, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // ---------------------------------------------------------------- phase field
@@ -700,15 +628,6 @@ __device__ __forceinline__ void d_phase_field(int lx, int ly, int lz, const floa
     if (!finite_f(dn)) dn = d_i;
     D[i] = dn;
     if (dn > 0.95f) fail[i] = 1;
-}
-__global__ void __launch_bounds__(kBlock) k_phase_field(int lx, int ly, int lz, const float* __restrict__ phi,
-                                                        const float* __restrict__ H, float* __restrict__ D,
-                                                        const float* __restrict__ Dold,
-                                                        const float* __restrict__ sigma,
-                                                        const uint8_t* __restrict__ type,
-                                                        uint8_t* __restrict__ fail, const float* __restrict__ hyd,
-                                                        float l0, float gc, float relax, int split) {
-    d_phase_field(lx, ly, lz, phi, H, D, Dold, sigma, type, fail, hyd, l0, gc, relax, split, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // ---------------------------------------------------------------- failure scan
@@ -781,23 +700,10 @@ __device__ __forceinline__ void d_failure_scan(int lx, int ly, int lz, const flo
     const int64_t mb = (x / kMacroBlock) + (int64_t)mbx * ((y / kMacroBlock) + (int64_t)mby * (z / kMacroBlock));
     atomicMax(macro + mb, __float_as_uint(res));
 }
-__global__ void __launch_bounds__(kBlock) k_failure_scan(int lx, int ly, int lz, const float* __restrict__ phi,
-                                                         const float* __restrict__ sigma,
-                                                         const float* __restrict__ rcomp,
-                                                         const uint8_t* __restrict__ type,
-                                                         uint8_t* __restrict__ fail,
-                                                         const float* __restrict__ rtens,
-                                                         uint32_t* __restrict__ macro,
-                                                         const float* __restrict__ rho, float phi_orphan) {
-    d_failure_scan(lx, ly, lz, phi, sigma, rcomp, type, fail, rtens, macro, rho, phi_orphan, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
-}
 
 __device__ __forceinline__ void d_macro_fill(uint32_t* __restrict__ macro, int64_t nmb, int64_t gt_, int64_t blk_) {
     const int64_t i = gt_;
     if (i < nmb) macro[i] = kMacroSeedBits;
-}
-__global__ void k_macro_fill(uint32_t* __restrict__ macro, int64_t nmb) {
-    d_macro_fill(macro, nmb, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // max over macro blocks as float (readbackMacroResidualMax, island_buffer.cpp:1012-1090),
@@ -817,10 +723,6 @@ __device__ __forceinline__ void d_macro_max(const uint32_t* __restrict__ macro, 
         for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_down_sync(0xffffffffu, s, o));
         if (threadIdx.x == 0) out[0] = s;
     }
-}
-__global__ void __launch_bounds__(kBlock) k_macro_max(const uint32_t* __restrict__ macro, int64_t nmb,
-                                                      float* __restrict__ out) {
-    d_macro_max(macro, nmb, out, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)blockIdx.x);
 }
 
 // ---------------------------------------------------------------- failure compaction
@@ -1073,6 +975,11 @@ __global__ void __launch_bounds__(kBlock) kb_phase_field(const CIsl* __restrict_
     d_phase_field(I.lx, I.ly, I.lz, I.phi, I.H, I.D, I.Dold, I.sigma, I.type, I.fail, I.hyd, l0, gc, relax, split,
                   t_, lb_);
 }
+__global__ void __launch_bounds__(kBlock) kb_take_phi(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                      int nisl) {
+    BATCH_ISLAND
+    if (I.phi_in && t_ < I.n) I.phi[t_] = I.phi_in[t_];
+}
 __global__ void __launch_bounds__(kBlock) kb_history(const CIsl* __restrict__ tab, const int* __restrict__ bs,
                                                      int nisl) {
     BATCH_ISLAND
@@ -1122,76 +1029,7 @@ namespace compat {
 
 int64_t fail_compact_blocks(int64_t n) { return ceil_div64(n, kCompactChunk); }
 
-void rbgs_color(cudaStream_t s, int lx, int ly, int lz, float* phi, const float* rho, const float* sigma,
-                const uint8_t* type, float* H, const uint32_t* macro, int color, float damping) {
-    const int cx = color & 1, cy = (color >> 1) & 1, cz = (color >> 2) & 1;
-    const int64_t nc = (int64_t)((lx - cx + 1) >> 1) * ((ly - cy + 1) >> 1) * ((lz - cz + 1) >> 1);
-    if (nc <= 0) return;
-    k_rbgs_color<<<grid_for(nc), kBlock, 0, s>>>(lx, ly, lz, phi, rho, sigma, type, H, macro, color, damping);
-}
-void jacobi_coarse(cudaStream_t s, int lx, int ly, int lz, float* phi_out, const float* phi_in, const float* rho,
-                   const float* sigma, const uint8_t* type, float* Hfine, float damping) {
-    const int64_t n = (int64_t)lx * ly * lz;
-    k_jacobi_coarse<<<grid_for(n), kBlock, 0, s>>>(lx, ly, lz, phi_out, phi_in, rho, sigma, type, Hfine, damping);
-}
-void restrict_level(cudaStream_t s, int fx, int fy, int fz, const float* phi_f, const float* rho_f,
-                    const float* sig_f, const uint8_t* type_f, int cx, int cy, int cz, float* phi_c, float* rho_c) {
-    const int64_t nc = (int64_t)cx * cy * cz;
-    k_restrict<<<grid_for(nc), kBlock, 0, s>>>(fx, fy, fz, phi_f, rho_f, sig_f, type_f, cx, cy, cz, phi_c, rho_c);
-}
-void prolong_level(cudaStream_t s, int fx, int fy, int fz, float* phi_f, int cx, int cy, int cz,
-                   const float* phi_c) {
-    const int64_t nf = (int64_t)fx * fy * fz;
-    k_prolong<<<grid_for(nf), kBlock, 0, s>>>(fx, fy, fz, phi_f, cx, cy, cz, phi_c);
-}
-void downsample(cudaStream_t s, int sx, int sy, int sz, const float* cond, const uint8_t* type, int dx, int dy,
-                int dz, float* out_cond, uint8_t* out_type) {
-    const int64_t dn = (int64_t)dx * dy * dz;
-    k_downsample<<<grid_for(dn), kBlock, 0, s>>>(sx, sy, sz, cond, type, dx, dy, dz, out_cond, out_type);
-}
-void pcg_precompute(cudaStream_t s, int lx, int ly, int lz, const float* sigma, float* invdiag) {
-    k_pcg_precompute<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, sigma, invdiag);
-}
 int64_t pcg_blocks(int64_t n) { return grid_for(n); }
-void pcg_matvec(cudaStream_t s, int lx, int ly, int lz, const float* in, float* out, const float* sigma,
-                const uint8_t* type, float* partial) {
-    k_pcg_matvec<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, in, out, sigma, type, partial);
-}
-void pcg_update(cudaStream_t s, int lx, int ly, int lz, float* phi, const float* r_in, float* r_out, float* p,
-                const float* ap, const float* src, const uint8_t* type, const float* sigma, const float* invdiag,
-                const float* red, int is_init, int64_t rtz_limit, float* partial) {
-    k_pcg_update<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, r_in, r_out, p, ap, src, type,
-                                                                    sigma, invdiag, red, is_init, rtz_limit,
-                                                                    partial);
-}
-void pcg_direction(cudaStream_t s, int lx, int ly, int lz, const float* r, float* p, const uint8_t* type,
-                   const float* red, const float* sigma) {
-    k_pcg_direction<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, r, p, type, red, sigma);
-}
-void finalize(cudaStream_t s, const float* partial, int64_t count, float* red, int slot, int rotate) {
-    k_finalize<<<1, kBlock, 0, s>>>(partial, count, red, slot, rotate);
-}
-void phase_field(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* H, float* D,
-                 const float* Dold, const float* sigma, const uint8_t* type, uint8_t* fail, const float* hyd,
-                 float l0, float gc, float relax, int split) {
-    k_phase_field<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, H, D, Dold, sigma, type, fail,
-                                                                     hyd, l0, gc, relax, split);
-}
-void history(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const uint8_t* type,
-             float* H) {
-    k_history<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, sigma, type, H);
-}
-void failure_scan(cudaStream_t s, int lx, int ly, int lz, const float* phi, const float* sigma, const float* rcomp,
-                  const uint8_t* type, uint8_t* fail, const float* rtens, uint32_t* macro, const float* rho) {
-    k_failure_scan<<<grid_for((int64_t)lx * ly * lz), kBlock, 0, s>>>(lx, ly, lz, phi, sigma, rcomp, type, fail,
-                                                                      rtens, macro, rho, kPhiOrphan);
-}
-void macro_fill(cudaStream_t s, uint32_t* macro, int64_t nmb) {
-    if (nmb > 0) k_macro_fill<<<grid_for(nmb), kBlock, 0, s>>>(macro, nmb);
-}
-void macro_max(cudaStream_t s, const uint32_t* macro, int64_t nmb, float* out) {
-    k_macro_max<<<1, kBlock, 0, s>>>(macro, nmb, out);
-}
 void fail_compact(cudaStream_t s, const uint8_t* fail, int lx, int ly, int lz, int ox, int oy, int oz,
                   int32_t* counts, int32_t* offsets, int32_t* total, int32_t* tuples, int32_t cap) {
     const int64_t n = (int64_t)lx * ly * lz;
@@ -1253,6 +1091,7 @@ void phase_field(cudaStream_t s, const BGroup& g, float l0, float gc, float rela
     BLAUNCH(kbN, kb_phase_field, l0, gc, relax, split);
 }
 void history(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_history); }
+void take_phi(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_take_phi); }
 void failure_scan(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_failure_scan); }
 void macro_max(cudaStream_t s, const BGroup& g) {
     if (g.nisl > 0) kb_macro_max<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab);

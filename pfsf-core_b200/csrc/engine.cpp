@@ -10,12 +10,14 @@
 // synchronisation per tick for all islands plus one for failure tuples.
 #include "engine.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
 #include "arena.h"
+#include "tick_batch.h"
 #include "compat.h"
 #include "kappa.h"
 
@@ -25,17 +27,6 @@ namespace pfsf_b200 {
 
 Island::Island() = default;
 Island::~Island() = default;
-
-namespace {
-inline int imax3(int a, int b, int c) { return std::max(a, std::max(b, c)); }
-inline int imin3(int a, int b, int c) { return std::min(a, std::min(b, c)); }
-inline float damping_of(int iter) { return iter >= kWarmupSteps ? kDampingFactor : 0.0f; }
-// r.z partial range of pcg_update (see oracle o_rtz_limit).
-inline int64_t rtz_limit(int64_t n) {
-    const int64_t g = (n + 511) / 512;
-    return std::min<int64_t>(n, 256 * g);
-}
-}  // namespace
 
 Engine::Engine(const pfsf_config& cfg) : cfg_(cfg) {
     if (const char* f = std::getenv("PFSF_FAULT_ALLOC_AFTER")) fault_alloc_after_ = std::atoll(f);
@@ -94,6 +85,7 @@ void Engine::shutdown() {
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
     free_arena();
+    free_tick_batch();
     for (auto& kv : islands_) free_island(*kv.second);
     islands_.clear();
     if (host_results_) cudaFreeHost(host_results_);
@@ -140,6 +132,7 @@ void Engine::free_island(Island& isl) {
     cudaStreamSynchronize(stream_);
     for (void* h : isl.host_registered) cudaHostUnregister(h);
     isl.host_registered.clear();
+    isl.host_pins.clear();
     int64_t freed = 0;
     for (auto& a : isl.allocations) { cudaFree(a.first); freed += (int64_t)a.second; }
     isl.allocations.clear();
@@ -183,14 +176,8 @@ pfsf_result Engine::add_island(const pfsf_island_desc* d) {
     // The reference allocates every per-island buffer here
     // (island_buffer.cpp:21-122).  Islands used only by the tolerance solve
     // never need the SoA-6 tick buffers, so those are allocated on first use
-    // (ensure_compat); a failure there is reported by the call that needed
-    // them.  The small per-island result record is allocated here so a
-    // device that cannot even hold that reports OUT_OF_VRAM at once.
-    isl->result = (TickResult*)dalloc(*isl, sizeof(TickResult));
-    if (!isl->result) {
-        free_island(*isl);
-        return PFSF_ERROR_OUT_OF_VRAM;
-    }
+    // (ensure_compat); a failure there is reported (PFSF_ERROR_OUT_OF_VRAM)
+    // by the call that needed them.
     islands_[d->island_id] = std::move(isl);
     return PFSF_OK;
 }
@@ -251,10 +238,31 @@ void Engine::mark_full_rebuild(int32_t id) {
     if (Island* s = find(id)) s->dirty = true;
 }
 
-static void try_pin(Island& s, void* p, int64_t bytes) {
-    if (!p || bytes <= 0) return;
-    if (cudaHostRegister(p, (size_t)bytes, cudaHostRegisterDefault) == cudaSuccess) s.host_registered.push_back(p);
-    else cudaGetLastError();  // pageable copies still work
+// Pins a caller-owned host array (mapped into the device address space) and
+// returns its device-visible address, or nullptr when it cannot be pinned
+// (the batched tick then copies it with cudaMemcpyAsync).  A range this
+// island pinned earlier (the stress buffer aliasing phi, a re-registration)
+// is looked up instead of pinned twice; ranges pinned by anyone else are not
+// used, since nothing here can tell how far their mapping reaches.
+const void* Engine::map_host(Island& s, void* p, int64_t bytes) {
+    if (!p || bytes <= 0) return nullptr;
+    const char* a = static_cast<const char*>(p);
+    for (const Island::HostPin& h : s.host_pins) {
+        const char* b = static_cast<const char*>(h.host);
+        if (a >= b && a + bytes <= b + h.bytes) return static_cast<const char*>(h.dev) + (a - b);
+    }
+    if (cudaHostRegister(p, (size_t)bytes, cudaHostRegisterMapped) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    s.host_registered.push_back(p);
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess || !d) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    s.host_pins.push_back(Island::HostPin{p, bytes, d});
+    return d;
 }
 
 pfsf_result Engine::register_buffers(int32_t id, const pfsf_island_buffers* b) {
@@ -279,6 +287,13 @@ pfsf_result Engine::register_buffers(int32_t id, const pfsf_island_buffers* b) {
     h.rtens = b->rtens_addr; h.rtens_bytes = b->rtens_bytes;
     h.max_phi = b->max_phi_addr; h.max_phi_bytes = b->max_phi_bytes;
     h.registered = true;
+    h.m_phi = map_host(*s, h.phi, 4 * n);
+    h.m_source = map_host(*s, h.source, 4 * n);
+    h.m_cond = map_host(*s, h.conductivity, 24 * n);
+    h.m_type = map_host(*s, h.voxel_type, n);
+    h.m_rcomp = map_host(*s, h.rcomp, 4 * n);
+    h.m_rtens = map_host(*s, h.rtens, 4 * n);
+    h.m_maxphi = map_host(*s, h.max_phi, 4 * n);
     if (!upload(*s)) return PFSF_ERROR_VULKAN;
     if (!CU_OK(cudaStreamSynchronize(stream_))) return PFSF_ERROR_VULKAN;
     s->dirty = true;
@@ -299,6 +314,7 @@ pfsf_result Engine::register_lookups(int32_t id, const pfsf_island_lookups* l) {
     s->hosts.curing = l->curing_addr;
     s->hosts.curing_bytes = l->curing_bytes;
     s->hosts.lookups_registered = true;
+    s->hosts.m_curing = map_host(*s, l->curing_addr, 4 * n);
     return PFSF_OK;
 }
 
@@ -309,6 +325,7 @@ pfsf_result Engine::register_stress(int32_t id, void* addr, int64_t bytes) {
     if (!s) return PFSF_ERROR_INVALID_ARG;
     s->hosts.stress_out = addr;
     s->hosts.stress_bytes = bytes;
+    s->hosts.m_stress = const_cast<void*>(map_host(*s, addr, std::min<int64_t>(bytes, 4 * s->n)));
     return PFSF_OK;
 }
 
@@ -366,144 +383,12 @@ bool Engine::ensure_pcg(Island& s) {
     return true;
 }
 
-// jacobi_solver.cpp:75-178: 8 colour passes, then chebyshev_iter++
-void Engine::rbgs_step(Island& s, float damping) {
-    for (int c = 0; c < 8; c++)
-        compat::rbgs_color(stream_, s.lx, s.ly, s.lz, s.phi, s.src, s.sigma, s.type, s.H, s.macro, c, damping);
-    launches_ += 8;
-    s.chebyshev_iter++;
-}
 
-void Engine::coarse_pass(Island& s, int level, float damping) {
-    if (level == 1) {
-        compat::jacobi_coarse(stream_, s.l1[0], s.l1[1], s.l1[2], s.phi1[1 - s.cur1], s.phi1[s.cur1], s.src1, s.sig1,
-                              s.type1, s.H, damping);
-        s.cur1 = 1 - s.cur1;
-    } else {
-        compat::jacobi_coarse(stream_, s.l2[0], s.l2[1], s.l2[2], s.phi2[1 - s.cur2], s.phi2[s.cur2], s.src2, s.sig2,
-                              s.type2, s.H, damping);
-        s.cur2 = 1 - s.cur2;
-    }
-    launches_++;
-}
 
-// dispatcher_vcycle.cpp:342-392 (W-cycle legs when L2 exists)
-int Engine::vcycle(Island& s) {
-    const float damping = damping_of(s.chebyshev_iter);
-    rbgs_step(s, damping);
-    compat::restrict_level(stream_, s.lx, s.ly, s.lz, s.phi, s.src, s.sigma, s.type, s.l1[0], s.l1[1], s.l1[2],
-                           s.phi1[s.cur1], s.src1);
-    launches_++;
-    if (s.n2 > 0) {
-        for (int leg = 0; leg < 2; leg++) {
-            coarse_pass(s, 1, damping);
-            coarse_pass(s, 1, damping);
-            compat::restrict_level(stream_, s.l1[0], s.l1[1], s.l1[2], s.phi1[s.cur1], s.src1, s.sig1, s.type1, s.l2[0],
-                                   s.l2[1], s.l2[2], s.phi2[s.cur2], s.src2);
-            launches_++;
-            for (int k = 0; k < 4; k++) coarse_pass(s, 2, damping);
-            compat::prolong_level(stream_, s.l1[0], s.l1[1], s.l1[2], s.phi1[s.cur1], s.l2[0], s.l2[1], s.l2[2],
-                                  s.phi2[s.cur2]);
-            launches_++;
-            coarse_pass(s, 1, damping);
-            coarse_pass(s, 1, damping);
-        }
-    } else {
-        for (int k = 0; k < 4; k++) coarse_pass(s, 1, damping);
-    }
-    compat::prolong_level(stream_, s.lx, s.ly, s.lz, s.phi, s.l1[0], s.l1[1], s.l1[2], s.phi1[s.cur1]);
-    launches_++;
-    rbgs_step(s, damping);
-    return 2;
-}
 
-// dispatcher.cpp:188-238
-bool Engine::try_vcycle(Island& s, int k, bool mg_available) {
-    const int maxd = imax3(s.lx, s.ly, s.lz), mind = imin3(s.lx, s.ly, s.lz);
-    int interval = kMgInterval;
-    if (mind > 0) {
-        const int ratio = maxd / mind;
-        if (ratio >= 8) interval = std::max(1, kMgInterval / 4);
-        else if (ratio >= 4) interval = std::max(1, kMgInterval / 2);
-    }
-    if (!(k > 0 && (k % interval) == 0 && mg_available)) return false;
-    if (!s.mg_alloc) {
-        if (!ensure_mg(s)) return false;
-        s.mg_dirty = true;
-    }
-    if (s.mg_dirty) {
-        // uploadMultigridData (island_buffer.cpp:600-776), on the device
-        compat::downsample(stream_, s.lx, s.ly, s.lz, s.sigma, s.type, s.l1[0], s.l1[1], s.l1[2], s.sig1, s.type1);
-        launches_++;
-        if (s.n2 > 0) {
-            compat::downsample(stream_, s.l1[0], s.l1[1], s.l1[2], s.sig1, s.type1, s.l2[0], s.l2[1], s.l2[2], s.sig2,
-                               s.type2);
-            launches_++;
-        }
-        s.mg_dirty = false;
-    }
-    vcycle(s);
-    if (mind > 0 && maxd >= 8 * mind) vcycle(s);
-    return true;
-}
 
-// dispatcher_pcg.cpp:254-272
-void Engine::pcg_initial(Island& s) {
-    compat::pcg_precompute(stream_, s.lx, s.ly, s.lz, s.sigma, s.invdiag);
-    compat::pcg_matvec(stream_, s.lx, s.ly, s.lz, s.phi, s.ap, s.sigma, s.type, nullptr);
-    compat::pcg_update(stream_, s.lx, s.ly, s.lz, s.phi, s.r[s.rcur], s.r[s.rcur], s.p, s.ap, s.src, s.type, s.sigma,
-                       s.invdiag, s.red, 1, rtz_limit(s.n), s.partial);
-    compat::finalize(stream_, s.partial, compat::pcg_blocks(s.n), s.red, 0, 0);
-    launches_ += 4;
-}
 
-// dispatcher_pcg.cpp:274-298 (matvec + p.Ap, update + r.z, direction, slot rotation)
-void Engine::pcg_step(Island& s, bool first) {
-    const int64_t nb = compat::pcg_blocks(s.n);
-    compat::pcg_matvec(stream_, s.lx, s.ly, s.lz, s.p, s.ap, s.sigma, s.type, s.partial);
-    compat::finalize(stream_, s.partial, nb, s.red, 1, first ? 0 : 1);
-    compat::pcg_update(stream_, s.lx, s.ly, s.lz, s.phi, s.r[s.rcur], s.r[1 - s.rcur], s.p, s.ap, s.src, s.type,
-                       s.sigma, s.invdiag, s.red, 0, rtz_limit(s.n), s.partial);
-    s.rcur = 1 - s.rcur;
-    compat::finalize(stream_, s.partial, nb, s.red, 2, 0);
-    compat::pcg_direction(stream_, s.lx, s.ly, s.lz, s.r[s.rcur], s.p, s.type, s.red, s.sigma);
-    launches_ += 5;
-}
 
-// dispatcher.cpp:106-186
-int Engine::solve_steps(Island& s, int steps) {
-    int recorded = 0;
-    const bool mg_available = cfg_.enable_multigrid && imax3(s.lx, s.ly, s.lz) > 4;
-    if (steps >= kPcgMinRbgs + kPcgMinSteps) {
-        const float prev = s.prev_macro, curr = s.last_macro;
-        const float ratio = (prev > 1e-10f) ? (curr / prev) : 0.0f;
-        const bool stalled = ratio > 0.95f;
-        if (stalled && pcg_enabled_ && !s.pcg_alloc) ensure_pcg(s);
-        const bool supports = pcg_enabled_ && s.n <= kPcgMaxN && s.pcg_alloc;
-        if (supports) {
-            const int maxr = std::max(kPcgMinRbgs, steps - kPcgMinSteps);
-            const int rb = stalled ? kPcgMinRbgs : maxr;
-            const int pc = steps - rb;
-            for (int k = 0; k < rb; k++) {
-                if (try_vcycle(s, k, mg_available)) continue;
-                rbgs_step(s, damping_of(s.chebyshev_iter));
-                recorded++;
-            }
-            pcg_initial(s);
-            for (int k = 0; k < pc; k++) {
-                pcg_step(s, k == 0);
-                recorded++;
-            }
-            return recorded;
-        }
-    }
-    for (int k = 0; k < steps; k++) {
-        if (try_vcycle(s, k, mg_available)) continue;
-        rbgs_step(s, damping_of(s.chebyshev_iter));
-        recorded++;
-    }
-    return recorded;
-}
 
 // pfsf_engine.cpp:424-600
 pfsf_result Engine::tick(const int32_t* ids, int32_t count, pfsf_tick_result* result, void* fail_addr,
@@ -520,21 +405,19 @@ pfsf_result Engine::tick(const int32_t* ids, int32_t count, pfsf_tick_result* re
     const int32_t legacy_cap = (result && result->events) ? result->capacity : 0;
     const int32_t want_cap = std::max(dbb_cap, legacy_cap);
 
+    // the dirty islands of the call, each once, in call order (the order of
+    // their failure tuples); the budget is checked while they are collected
     std::vector<Island*> dispatched;
     for (int32_t k = 0; k < count; k++) {
         Island* s = find(ids[k]);
         if (!s || !s->dirty) continue;
+        if (std::find(dispatched.begin(), dispatched.end(), s) != dispatched.end()) continue;
         if (!ensure_compat(*s)) return PFSF_ERROR_OUT_OF_VRAM;
-        if (s->hosts.registered && !upload(*s)) return PFSF_ERROR_VULKAN;
         const auto el = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0);
         if (el.count() >= cfg_.tick_budget_ms) break;
-
-        compat::macro_fill(stream_, s->macro, s->nmb);
-        launches_++;
-        solve_steps(*s, kStepsMajor);
-        if (pfsf_result rc = enqueue_tail(*s, want_cap); rc != PFSF_OK) return rc;
         dispatched.push_back(s);
     }
+    if (pfsf_result rc = tick_batched(dispatched, want_cap); rc != PFSF_OK) return rc;
     if (pfsf_result rc = finish_dispatch(dispatched, drain, fail_addr, dbb_count, dbb_cap, result, legacy_cap);
         rc != PFSF_OK)
         return rc;
@@ -546,55 +429,15 @@ pfsf_result Engine::tick(const int32_t* ids, int32_t count, pfsf_tick_result* re
     return PFSF_OK;
 }
 
-// The reference tick's tail on the island's current phi: phase field (with
-// its D snapshot), failure scan, macro-residual max, failure compaction into
-// device tuples, stress readback (pfsf_engine.cpp:513-560).
-pfsf_result Engine::enqueue_tail(Island& is, int32_t want_cap) {
-    Island* s = &is;
-    if (cfg_.enable_phase_field) {
-        cudaMemcpyAsync(s->Dold, s->D, (size_t)s->n * 4, cudaMemcpyDeviceToDevice, stream_);
-        compat::phase_field(stream_, s->lx, s->ly, s->lz, s->phi, s->H, s->D, s->Dold, s->sigma, s->type, s->fail,
-                            s->hyd, kPfL0, kPfGc, kPfRelax, 1);
-        launches_++;
-    }
-    compat::failure_scan(stream_, s->lx, s->ly, s->lz, s->phi, s->sigma, s->rcomp, s->type, s->fail, s->rtens,
-                         s->macro, s->src);
-    compat::macro_max(stream_, s->macro, s->nmb, &s->result->macro_max);
-    launches_ += 2;
-    if (want_cap > 0) {
-        if (s->tuple_cap < want_cap) {
-            s->tuples = (int32_t*)dalloc(*s, (size_t)want_cap * 16);
-            if (!s->tuples) return PFSF_ERROR_OUT_OF_VRAM;
-            s->tuple_cap = want_cap;
-        }
-        compat::fail_compact(stream_, s->fail, s->lx, s->ly, s->lz, s->origin.x, s->origin.y, s->origin.z,
-                             s->fcounts, s->foffsets, &s->result->fail_total, s->tuples, want_cap);
-        launches_ += 3;
-    }
-    if (s->hosts.stress_out && s->hosts.stress_bytes > 0) {
-        const int64_t nf = std::min<int64_t>(s->n, s->hosts.stress_bytes / 4);
-        if (!CU_OK(cudaMemcpyAsync(s->hosts.stress_out, s->phi, (size_t)nf * 4, cudaMemcpyDeviceToHost, stream_)))
-            return PFSF_ERROR_VULKAN;
-    }
-    return PFSF_OK;
-}
 
-// Reads the dispatched islands' tick results back and appends their failure
+// After tick_batched queued the dispatched islands' tick results into
+// host_results_ (dispatch order): reads them and appends their failure
 // tuples to the caller's buffers in island order, voxel order
 // (island_buffer.cpp:864-966).
 pfsf_result Engine::finish_dispatch(const std::vector<Island*>& dispatched, bool drain, void* fail_addr,
                                     int32_t dbb_count, int32_t dbb_cap, pfsf_tick_result* result,
                                     int32_t legacy_cap) {
     if (!dispatched.empty()) {
-        if ((int)dispatched.size() > host_results_cap_) {
-            cudaFreeHost(host_results_);
-            host_results_cap_ = (int)dispatched.size() * 2;
-            if (!CU_OK(cudaMallocHost((void**)&host_results_, sizeof(TickResult) * host_results_cap_)))
-                return PFSF_ERROR_VULKAN;
-        }
-        for (size_t k = 0; k < dispatched.size(); k++)
-            cudaMemcpyAsync(&host_results_[k], dispatched[k]->result, sizeof(TickResult), cudaMemcpyDeviceToHost,
-                            stream_);
         if (!CU_OK(cudaStreamSynchronize(stream_))) return PFSF_ERROR_VULKAN;
         // failure tuples in island order, voxel order (island_buffer.cpp:864-966)
         int32_t legacy_count = 0;

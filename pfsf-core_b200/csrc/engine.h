@@ -55,6 +55,11 @@ struct HostBuffers {
     void* k_source = nullptr;
     void* k_kappa = nullptr;
     void* k_type = nullptr;
+    // device-visible mappings of the pinned reference-layout arrays (nullptr:
+    // the array could not be pinned and is copied with cudaMemcpyAsync)
+    const void *m_phi = nullptr, *m_source = nullptr, *m_cond = nullptr, *m_type = nullptr, *m_rcomp = nullptr,
+               *m_rtens = nullptr, *m_maxphi = nullptr, *m_curing = nullptr;
+    void* m_stress = nullptr;
     // adjoint buffers (pfsf_register_island_adjoint)
     bool adjoint_registered = false;
     const void* a_grad_phi = nullptr;
@@ -62,7 +67,8 @@ struct HostBuffers {
     void* a_grad_kappa = nullptr;
 };
 
-// Small device-side per-island tick result, read back in one copy.
+// Per-island tick result (device records of the batched tick, read back in
+// one copy).
 struct TickResult {
     float macro_max;
     int32_t fail_total;
@@ -84,7 +90,6 @@ struct Island {
           *maxphi = nullptr, *hyd = nullptr, *H = nullptr, *D = nullptr, *Dold = nullptr;
     uint8_t *type = nullptr, *fail = nullptr;
     uint32_t* macro = nullptr;
-    TickResult* result = nullptr;
     int32_t *fcounts = nullptr, *foffsets = nullptr, *tuples = nullptr;
     int32_t tuple_cap = 0;
 
@@ -115,6 +120,12 @@ struct Island {
 
     std::vector<std::pair<void*, size_t>> allocations;  // device allocations owned by this island
     std::vector<void*> host_registered;
+    struct HostPin {
+        const void* host;
+        int64_t bytes;
+        const void* dev;
+    };
+    std::vector<HostPin> host_pins;  // ranges pinned by map_host and their device addresses
     Island();
     ~Island();
 };
@@ -171,6 +182,18 @@ public:
     Island* find(int32_t id);
 
 private:
+    struct TickBatch;
+    // One tick of the reference schedule for every island in `set` (all
+    // dirty, compat buffers allocated): islands grouped by schedule, each
+    // schedule step one launch per group, the whole tick replayed from a
+    // CUDA graph while the group structure stays the same (engine_batch.cpp).
+    // With phi_in (one device pointer per island of `set`) it runs the
+    // tolerance tick's tail instead: phi taken from phi_in, the history
+    // update, then the same tail; islands not dirty are not re-uploaded.
+    pfsf_result tick_batched(const std::vector<Island*>& set, int32_t want_cap,
+                             const std::vector<const float*>* phi_in = nullptr);
+    void free_tick_batch();
+    const void* map_host(Island& s, void* p, int64_t bytes);
     bool ensure_compat(Island& isl);
     bool build_arena(const std::vector<Island*>& set);
     void free_arena();
@@ -180,19 +203,11 @@ private:
     bool grid_barrier_failed() const;
     void destroy_side();
     void fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_solve_stats& st) const;
-    pfsf_result enqueue_tail(Island& isl, int32_t want_cap);
     pfsf_result finish_dispatch(const std::vector<Island*>& dispatched, bool drain, void* fail_addr, int32_t dbb_count,
                                 int32_t dbb_cap, pfsf_tick_result* result, int32_t legacy_cap);
     bool upload(Island& isl);
     bool ensure_mg(Island& isl);
     bool ensure_pcg(Island& isl);
-    void rbgs_step(Island& isl, float damping);
-    int vcycle(Island& isl);
-    bool try_vcycle(Island& isl, int k, bool mg_available);
-    void coarse_pass(Island& isl, int level, float damping);
-    void pcg_initial(Island& isl);
-    void pcg_step(Island& isl, bool first);
-    int solve_steps(Island& isl, int steps);
     void free_island(Island& isl);
 
     pfsf_config cfg_;
@@ -213,6 +228,8 @@ private:
     float last_tick_ms_ = 0.0f;
     TickResult* host_results_ = nullptr;  // pinned
     int host_results_cap_ = 0;
+
+    std::unique_ptr<TickBatch> tbatch_;
 
     // tolerance-solve arena (one packed allocation for a set of islands)
     struct Arena;

@@ -556,7 +556,6 @@ pfsf_result Engine::tick_tolerance(const int32_t* ids, int32_t count, void* fail
     for (Island* s : set) {
         if (!s->hosts.registered) return PFSF_ERROR_INVALID_ARG;
         if (!ensure_compat(*s)) return PFSF_ERROR_OUT_OF_VRAM;
-        if (s->dirty && !upload(*s)) return PFSF_ERROR_VULKAN;  // as pfsf_tick_dbb: dirty islands re-upload
         sids.push_back(s->id);
     }
     pfsf_solve_stats st{};
@@ -567,17 +566,12 @@ pfsf_result Engine::tick_tolerance(const int32_t* ids, int32_t count, void* fail
     }
     if (pfsf_result rc = solve_to_tolerance(sids.data(), (int32_t)sids.size(), tol, max_iter, 0, &st); rc != PFSF_OK)
         return rc;
-    const Arena& A = *arena_;
-    for (size_t q = 0; q < set.size(); q++) {
-        Island* s = set[q];
-        if (!CU_OK(cudaMemcpyAsync(s->phi, A.dev.e + A.desc[q].off, (size_t)s->n * 4, cudaMemcpyDeviceToDevice,
-                                   stream_)))
-            return PFSF_ERROR_VULKAN;
-        compat::macro_fill(stream_, s->macro, s->nmb);
-        compat::history(stream_, s->lx, s->ly, s->lz, s->phi, s->sigma, s->type, s->H);
-        launches_ += 2;
-        if (pfsf_result rc = enqueue_tail(*s, dbb_cap); rc != PFSF_OK) return rc;
-    }
+    // the tail over all islands in one batched pass: dirty islands' reference
+    // buffers uploaded (as pfsf_tick_dbb does), phi taken from the arena,
+    // H = max(H, psi_e(phi)), phase field, failure scan and compaction
+    std::vector<const float*> phi_in;
+    for (size_t q = 0; q < set.size(); q++) phi_in.push_back(arena_->dev.e + arena_->desc[q].off);
+    if (pfsf_result rc = tick_batched(set, dbb_cap, &phi_in); rc != PFSF_OK) return rc;
     if (pfsf_result rc = finish_dispatch(set, drain, fail_addr, 0, dbb_cap, nullptr, 0); rc != PFSF_OK) return rc;
     if (out) *out = st;
     return PFSF_OK;

@@ -1,0 +1,33 @@
+// State of the batched reference tick (engine_batch.cpp).
+#pragma once
+#include <vector>
+
+#include "compat.h"
+#include "engine.h"
+
+namespace pfsf_b200 {
+
+// What recording one group's schedule does to the per-island state: rbgs
+// steps counted (chebyshev_iter), coarse ping-pong flips, PCG slot flips,
+// whether a V-cycle rebuilt the coarse inputs.
+struct TickEffect {
+    int steps = 0, f1 = 0, f2 = 0, fr = 0, downsampled = 0;
+};
+
+struct Engine::TickBatch {
+    // device: descriptor table, block prefixes (per group, then the whole
+    // set), result records; pinned host staging of the table and prefixes
+    compat::CIsl* d_tab = nullptr;
+    int* d_bs = nullptr;
+    TickResult* d_res = nullptr;
+    compat::CIsl* h_tab = nullptr;
+    int* h_bs = nullptr;
+    int cap_isl = 0, cap_bs = 0;
+    // captured tick and the structure it was captured for
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int64_t> key;
+    int64_t graph_launches = 0;
+    std::vector<TickEffect> effects;  // per group of the captured structure
+};
+
+}  // namespace pfsf_b200

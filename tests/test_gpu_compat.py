@@ -59,13 +59,17 @@ def _tick_both(eng, iid, host, ref, origin, cap=4096):
 
 
 def _assert_tick_parity(eng, iid, host, ref, fb, want, t):
+    assert fb[0] == want[0], f"tick {t}: failure count {fb[0]} vs {want[0]}"
+    assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]]), f"tick {t}: failure tuples"
+    _assert_island_state(eng, iid, host, ref, t)
+
+
+def _assert_island_state(eng, iid, host, ref, t):
     phi_ref = ref.view("phi")
     scale = max(float(np.abs(phi_ref).max()), 1e-30)
     err = float(np.abs(host["phi"].astype(np.float64) - phi_ref).max()) / scale
     assert err <= PHI_TOL, f"tick {t}: phi rel err {err:.3e}"
     assert np.array_equal(eng.debug_field(iid, 3), ref.view("fail").astype(np.uint8)), f"tick {t}: fail flags"
-    assert fb[0] == want[0], f"tick {t}: failure count {fb[0]} vs {want[0]}"
-    assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]]), f"tick {t}: failure tuples"
     for field, name in ((1, "H"), (2, "D")):
         g = eng.debug_field(iid, field)
         r = ref.view(name)
@@ -153,6 +157,44 @@ def test_multi_island_tick_order(eng):
     r2.failures(o2, capacity=cap, dbb=want)
     assert fb[0] == want[0] and fb[0] > 0
     assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]])
+
+
+def test_batched_tick_many_islands(eng):
+    """Two dozen islands of different shapes and schedules (plain RBGS, PCG
+    after a stall, V-cycles every 4 / 2 / 1 steps, none) in one
+    pfsf_tick_dbb call per tick: every island matches its own oracle island
+    each tick, the failure buffer holds the islands' tuples in call order,
+    and the kernel launches of a tick do not grow with the island count (one
+    launch per schedule step and island group, replayed from a CUDA graph)."""
+    names = ["block8", "noise20", "slab", "rod", "tiny", "block16"]
+    isl = []
+    for k in range(24):
+        c = cases.compat_case(names[k % len(names)])
+        if k % 4 == 1:
+            c["rcomp"][::5] = 1e-9
+        origin = (40 * k, -3 * k, k)
+        iid, host, ref = _setup(eng, c, origin)
+        isl.append((iid, host, ref, origin))
+    ids = [x[0] for x in isl]
+    cap = 1 << 15
+    per_tick = []
+    for t in range(5):
+        for iid in ids:
+            eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+        fb = np.zeros(1 + 4 * cap, np.int32)
+        l0 = eng.launches()
+        assert eng.tick_dbb(ids, fb) == capi.PFSF_OK
+        per_tick.append(eng.launches() - l0)
+        want = np.zeros(1 + 4 * cap, np.int32)
+        for iid, host, ref, origin in isl:
+            ref.tick()
+            ref.failures(origin, capacity=cap, dbb=want)
+        assert fb[0] == want[0] and fb[0] > 0, (t, fb[0], want[0])
+        assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]]), f"tick {t}: failure tuples"
+        for iid, host, ref, origin in isl:
+            _assert_island_state(eng, iid, host, ref, t)
+    # 24 islands one at a time would take ~24 x 200 launches per tick
+    assert max(per_tick) < 1500, per_tick
 
 
 def test_reference_fixtures_parity(eng):

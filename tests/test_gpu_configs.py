@@ -18,7 +18,8 @@ phi rounded to FP32.  Checks:
   history update, flux_in > 3 flux_out, scales psi_e by 100), sits within
   the solve tolerance of a decision threshold; since the phase field reads
   the damage of the six face neighbours, the margin grows by one voxel per
-  tick.  The number of margin voxels is reported and bounded;
+  tick.  The number of margin voxels is reported and bounded (0.5 % of the
+  grid after one tick, 2 % after three);
 * H and damage: within 1e-5 of their maxima outside the same margin.
 
 Config 1: the 32^3 fully solid block, three-material mix.  Config 2: the
@@ -172,18 +173,18 @@ def test_config1_solid_block_32(eng, prec):
     isl = synth.solid_block((32, 32, 32), seed=1)
     rep = _run(eng, 9300 + prec, isl, _case(isl), ticks=1, prec=prec, origin=(4, 0, -2))
     assert rep[0]["failures"] > 0
-    assert rep[0]["margin_voxels"] <= isl.n // 1000, rep
+    assert rep[0]["margin_voxels"] <= isl.n // 200, rep
 
 
 def test_config2_noise_256x256x128(eng):
     isl = synth.noise_island((256, 256, 128), seed=11)
     rep = _run(eng, 9310, isl, _case(isl), ticks=1, prec=capi.PREC_BF16)
     assert rep[0]["failures"] > 0
-    assert rep[0]["margin_voxels"] <= isl.n // 1000, rep
+    assert rep[0]["margin_voxels"] <= isl.n // 200, rep
 
 
 def test_config5_fracture_reduced(eng):
     isl = synth.noise_island((128, 128, 64), seed=51, occupancy=0.55)
     rep = _run(eng, 9320, isl, _case(isl), ticks=3, prec=capi.PREC_BF16, ramp=2.0)
     assert rep[-1]["failures"] >= rep[0]["failures"] > 0
-    assert max(r["margin_voxels"] for r in rep) <= isl.n // 100, rep
+    assert max(r["margin_voxels"] for r in rep) <= isl.n // 50, rep
