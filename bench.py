@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch", "single", "adjoint", "fracture"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "single", "adjoint", "fracture", "tick_dbb"], default="batch")
     ap.add_argument("--ticks", type=int, default=200, help="fracture workload: ticks")
     ap.add_argument("--fd-voxels", type=int, default=256)
     ap.add_argument("--dims", default="256,256,128", help="single workload: island sides x,y,z")
@@ -673,6 +673,92 @@ def run_fracture(args):
     eng.close()
 
 
+def run_tick_dbb(args):
+    """The drop-in reference tick (pfsf_tick_dbb: the fixed 16-step adaptive
+    RBGS / PCG / V-cycle schedule, phase field, failure scan, failure
+    compaction, stress readback) over the batch workload's islands, every
+    island dirty every tick as the Java runtime marks them
+    (NativePFSFRuntime.java:289), so every tick also uploads every island's
+    arrays from the caller's pinned host buffers.  Face conductivity = the
+    kappa link value; loads x 1e-4 so phi stays in the range the reference
+    clamps to (phi <= 1e7).  value = device time of a tick (CUDA events on
+    the engine stream, upload included); e2e = wall time of the call."""
+    from pfsf_b200 import capi
+    isls, meta = make_workload(args, 0)
+    t0 = time.perf_counter()
+    host = []
+    for isl in isls:
+        host.append({"phi": np.zeros(isl.n, np.float32), "source": (isl.source * np.float32(1e-4)).astype(np.float32),
+                     "cond": synth_face_sigma(isl), "type": isl.vtype, "rcomp": isl.rcomp.astype(np.float32),
+                     "rtens": isl.rtens.astype(np.float32), "max_phi": np.full(isl.n, 1e9, np.float32)})
+    t_gen = time.perf_counter() - t0
+    import torch
+    eng = capi.Engine(capi.default_config(max_island_size=1 << 28, tick_budget_ms=1 << 30, vram=180 << 30))
+    if eng.init() != capi.PFSF_OK:
+        raise RuntimeError("pfsf_init failed")
+    ids = []
+    for k, (isl, h) in enumerate(zip(isls, host)):
+        iid = k + 1
+        assert eng.add_island(iid, isl.dims, (0, 0, 128 * k)) == capi.PFSF_OK
+        assert eng.register_buffers(iid, h["phi"], h["source"], h["cond"], h["type"], h["rcomp"], h["rtens"],
+                                    h["max_phi"]) == capi.PFSF_OK
+        assert eng.register_stress(iid, h["phi"]) == capi.PFSF_OK
+        ids.append(iid)
+    cap = 1024  # the Java runtime's failure buffer: 4 + 1024 x 16 bytes (NativePFSFRuntime.java:251-252)
+    fb = np.zeros(1 + 4 * cap, np.int32)
+
+    def tick():
+        for iid in ids:
+            eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+        rc = eng.tick_dbb(ids, fb)
+        if rc != capi.PFSF_OK:
+            raise RuntimeError(f"pfsf_tick_dbb rc={rc}")
+        rc, rep = eng.tick_report()
+        return rep
+
+    for _ in range(max(args.warmup, 1)):
+        tick()
+    reps, walls = [], []
+    with Clocks(0) as clk:
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            reps.append(tick())
+            walls.append((time.perf_counter() - t1) * 1000.0)
+    dev_ms = float(np.mean([r.device_ms for r in reps]))
+    bytes_ = float(np.mean([r.algorithmic_bytes for r in reps]))
+    peak, peak_kind = peaks()
+    h2d = sum(isl.n * (4 + 4 + 24 + 1 + 4 + 4 + 4) for isl in isls)
+    d2h = sum(isl.n * 4 for isl in isls) + 4 + 16 * int(fb[0])
+    line = {
+        "metric": "drop-in reference tick (pfsf_tick_dbb) ms/tick", "value": dev_ms, "unit": "ms/tick",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+        "data": "synthetic", "dtype": "f32",
+        "config": {"workload": (f"{len(isls)} islands (log-uniform sides, scale {meta['scale']:.3f}), "
+                                f"{meta['grid_total']} grid / {meta['active_total']} active voxels, all dirty every "
+                                f"tick, 16-step reference schedule"), "islands": len(isls),
+                   "grid_voxels": meta["grid_total"], "active_voxels": meta["active_total"],
+                   "generation_s": t_gen},
+        "e2e": {"value": float(np.mean(walls)), "unit": "ms/tick", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": bytes_ / (dev_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": bytes_ / (dev_ms * 1e-3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                     "algorithmic_bytes": bytes_, "kernel": "the tick's graph (dominant: kb_rbgs_color)",
+                     "note": ("model bytes of every pass (pfsf_last_tick_report) over the tick's stream time, "
+                              "which includes the zero-copy upload of every island's arrays over the host link")},
+        "voxel_updates_per_s": 16.0 * meta["grid_total"] / (dev_ms * 1e-3),
+        "gpu_launches": int(np.mean([r.kernel_launches for r in reps])),
+        "groups": int(reps[-1].groups), "graph_replayed": int(reps[-1].graph_replayed),
+        "failures_last_tick": int(fb[0]), "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def synth_face_sigma(isl):
+    from pfsf_b200 import synth
+    return synth.face_sigma_from_kappa(isl.dims, isl.vtype, isl.kappa)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -681,6 +767,8 @@ def main():
         run_adjoint(args)
     elif args.workload == "fracture":
         run_fracture(args)
+    elif args.workload == "tick_dbb":
+        run_tick_dbb(args)
     else:
         run_ours(args)
 

@@ -134,6 +134,27 @@ typedef struct pfsf_island_report {
 
 PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine engine, int32_t island_id, pfsf_island_report* out);
 
+/* No counterpart in the reference ABI.  Shape of the last reference tick
+ * (pfsf_tick_dbb / pfsf_tick) or tolerance-tick tail: the dispatched islands
+ * run as groups of equal schedule, each schedule step one kernel launch over
+ * its group, the whole launch sequence replayed from a CUDA graph while the
+ * group structure is unchanged.  INVALID_ARG before the first tick. */
+typedef struct pfsf_tick_report {
+    int32_t struct_bytes;
+    int32_t islands;           /* islands dispatched */
+    int32_t groups;            /* schedule groups */
+    int32_t graph_replayed;    /* 1: the captured launch sequence was reused */
+    int64_t kernel_launches;   /* kernels the tick launched */
+    double algorithmic_bytes;  /* device-memory bytes of the tick's passes: every
+                                  array a pass touches counted once per pass */
+    double grid_voxels;        /* voxels of the dispatched islands' boxes */
+    float device_ms;           /* engine-stream time from the table upload to the
+                                  result copy (CUDA events) */
+    int32_t reserved;
+} pfsf_tick_report;
+
+PFSF_API pfsf_result pfsf_last_tick_report(pfsf_engine engine, pfsf_tick_report* out);
+
 /* Copies the FP64 solution accumulator of the last tolerance solve of an
  * island (count = min(N, capacity) values).  The FP32 phi written back by
  * pfsf_solve_to_tolerance is this vector rounded to float32. */

@@ -169,6 +169,7 @@ public:
     pfsf_result adjoint_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter,
                                      uint32_t flags, pfsf_solve_stats* out);
     pfsf_result debug_read_field(int32_t id, int32_t field, void* out, int64_t bytes, int64_t* out_bytes);
+    pfsf_result last_tick_report(pfsf_tick_report* out) const;
 
     cudaStream_t stream() const { return stream_; }
     int num_sms() const { return num_sms_; }

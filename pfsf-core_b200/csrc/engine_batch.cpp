@@ -45,15 +45,64 @@ struct Plan {
     bool operator==(const Plan& o) const { return std::memcmp(this, &o, sizeof(Plan)) == 0; }
 };
 
+// Device-memory bytes of one island's tick: every array a pass touches
+// counted once per pass, per fine voxel (n) or coarse cell (n1, n2).  An RBGS
+// colour sweep or coarse Jacobi pass moves the SoA-6 conductivity (24 B),
+// phi in and out (8), the source (4), the type (1) and H read and written
+// (8): 45 B per cell.
+double tick_bytes(const Island& s, const Plan& p, bool tail_only, bool phase, bool compact, bool uploaded,
+                  bool stress) {
+    const double n = (double)s.n, n1 = (double)s.n1, n2 = (double)s.n2;
+    const double sweep = 45.0;
+    double b = 0.0;
+    if (tail_only) {
+        b += 8.0 * n + 37.0 * n;  // phi taken from the solve; history update
+    } else {
+        const double vc = 2.0 * sweep * n + 33.0 * n + 8.0 * n1 +
+                          2.0 * (4.0 * sweep * n1 + 33.0 * n1 + 8.0 * n2 + 4.0 * sweep * n2 + 8.0 * n1 + 4.0 * n2) +
+                          8.0 * n + 4.0 * n1;
+        int vcycles = 0, sweeps = 0;
+        for (int k = 0; k < p.rb; k++) {
+            if (p.mg && k > 0 && (k % p.interval) == 0) vcycles += p.extra ? 2 : 1;
+            else sweeps++;
+        }
+        b += sweeps * sweep * n + vcycles * vc;
+        if (p.mg_dirty) b += 25.0 * n + 50.0 * n1 + 25.0 * n2;
+        if (p.pcg) b += (28.0 + 33.0 + 41.0) * n + p.pc * (33.0 + 53.0 + 37.0) * n;
+    }
+    if (phase) b += 8.0 * n + 47.0 * n;
+    b += 42.0 * n;               // failure scan
+    if (compact) b += 2.0 * n;   // compaction reads the flags twice
+    if (uploaded) b += 45.0 * n; // the uploaded arrays written into HBM
+    if (stress) b += 4.0 * n;    // phi read for the stress readback
+    return b;
+}
+
 inline int imax3(int a, int b, int c) { return std::max(a, std::max(b, c)); }
 inline int imin3(int a, int b, int c) { return std::min(a, std::min(b, c)); }
 
 }  // namespace
 
+pfsf_result Engine::last_tick_report(pfsf_tick_report* out) const {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (!out || !tbatch_ || !tbatch_->have_tick) return PFSF_ERROR_INVALID_ARG;
+    pfsf_tick_report r = tbatch_->last;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, tbatch_->ev0, tbatch_->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        ms = -1.0f;
+    }
+    r.device_ms = ms;
+    *out = r;
+    return PFSF_OK;
+}
+
 void Engine::free_tick_batch() {
     if (!tbatch_) return;
     TickBatch& B = *tbatch_;
     cudaStreamSynchronize(stream_);
+    if (B.ev0) cudaEventDestroy(B.ev0);
+    if (B.ev1) cudaEventDestroy(B.ev1);
     if (B.exec) cudaGraphExecDestroy(B.exec);
     if (B.d_tab) cudaFree(B.d_tab);
     if (B.d_bs) cudaFree(B.d_bs);
@@ -79,10 +128,12 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
     for (int k = 0; k < nisl; k++) {
         Island& s = *set[k];
         Plan p{};
-        if (want_cap > 0 && s.tuple_cap < want_cap) {
-            s.tuples = (int32_t*)dalloc(s, (size_t)want_cap * 16);
+        // an island cannot fail more voxels than it has
+        const int32_t need = (int32_t)std::min<int64_t>(want_cap, s.n);
+        if (need > 0 && s.tuple_cap < need) {
+            s.tuples = (int32_t*)dalloc(s, (size_t)need * 16);
             if (!s.tuples) return PFSF_ERROR_OUT_OF_VRAM;
-            s.tuple_cap = want_cap;
+            s.tuple_cap = need;
         }
         if (tail_only) {
             if (uploads(s)) s.mg_dirty = true;
@@ -180,7 +231,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
         c.res_fail = &B.d_res[k].fail_total;
         c.fcounts = s.fcounts; c.foffsets = s.foffsets;
         c.tuples = want_cap > 0 ? s.tuples : nullptr;
-        c.tuple_cap = want_cap;
+        c.tuple_cap = (int32_t)std::min<int64_t>(want_cap, s.n);
         c.iter0 = s.chebyshev_iter;
         c.cur1 = s.cur1; c.cur2 = s.cur2; c.rcur = s.rcur;
         if (plan[k].mg) {
@@ -254,6 +305,8 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
         key.insert(key.end(), {(int64_t)c.lx, (int64_t)c.ly, (int64_t)c.lz, c.h_phi ? 1 : 0, c.h_stress ? 1 : 0});
     }
 
+    if (!B.ev0 && (!CU_OK(cudaEventCreate(&B.ev0)) || !CU_OK(cudaEventCreate(&B.ev1)))) return PFSF_ERROR_VULKAN;
+    cudaEventRecord(B.ev0, stream_);
     bool ok = CU_OK(cudaMemcpyAsync(B.d_tab, B.h_tab, sizeof(compat::CIsl) * nisl, cudaMemcpyHostToDevice, stream_));
     ok &= CU_OK(cudaMemcpyAsync(B.d_bs, B.h_bs, sizeof(int) * bo, cudaMemcpyHostToDevice, stream_));
     // islands whose arrays could not be pinned: uploaded by copies
@@ -267,6 +320,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
         cudaGraphExecDestroy(B.exec);
         B.exec = nullptr;
     }
+    const bool replayed = B.exec != nullptr;
     if (!B.exec) {
         // ---- record the tick once, under capture
         B.effects.assign(ng, TickEffect{});
@@ -405,6 +459,21 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
     // results (call order) in one copy; finish_dispatch reads them after its sync
     if (!CU_OK(cudaMemcpyAsync(host_results_, B.d_res, sizeof(TickResult) * nisl, cudaMemcpyDeviceToHost, stream_)))
         return PFSF_ERROR_VULKAN;
+    cudaEventRecord(B.ev1, stream_);
+    pfsf_tick_report& R = B.last;
+    R = pfsf_tick_report{};
+    R.struct_bytes = (int32_t)sizeof(R);
+    R.islands = nisl;
+    R.groups = tail_only ? 1 : ng;
+    R.graph_replayed = replayed ? 1 : 0;
+    R.kernel_launches = B.graph_launches;
+    for (int j = 0; j < nisl; j++) {
+        const Island& s = *set[order[j]];
+        R.algorithmic_bytes += tick_bytes(s, plan[order[j]], tail_only, cfg_.enable_phase_field, want_cap > 0,
+                                          B.h_tab[j].h_phi != nullptr, B.h_tab[j].h_stress != nullptr);
+        R.grid_voxels += (double)s.n;
+    }
+    B.have_tick = true;
 
     // ---- per-island schedule state after the tick
     for (int q = 0; q < ng; q++) {

@@ -181,6 +181,11 @@ PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine e, int32_t id, pfsf_is
     return g ? g->island_report(id, out) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_last_tick_report(pfsf_engine e, pfsf_tick_report* out) {
+    Engine* g = E(e);
+    return g ? g->last_tick_report(out) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_read_solution64(pfsf_engine e, int32_t id, double* out, int64_t cap, int64_t* count) {
     Engine* g = E(e);
     return g ? g->read_solution64(id, out, cap, count) : PFSF_ERROR_INVALID_ARG;

@@ -28,6 +28,10 @@ struct Engine::TickBatch {
     std::vector<int64_t> key;
     int64_t graph_launches = 0;
     std::vector<TickEffect> effects;  // per group of the captured structure
+    // the last tick (pfsf_last_tick_report); the events bracket its stream work
+    bool have_tick = false;
+    pfsf_tick_report last{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 }  // namespace pfsf_b200

@@ -100,6 +100,12 @@ class IslandReport(C.Structure):
                 ("precond_ms", C.c_double)]
 
 
+class TickReport(C.Structure):
+    _fields_ = [("struct_bytes", C.c_int32), ("islands", C.c_int32), ("groups", C.c_int32),
+                ("graph_replayed", C.c_int32), ("kernel_launches", C.c_int64), ("algorithmic_bytes", C.c_double),
+                ("grid_voxels", C.c_double), ("device_ms", C.c_float), ("reserved", C.c_int32)]
+
+
 _lib = None
 
 
@@ -154,6 +160,7 @@ def load():
         "pfsf_compact_failures_noalloc": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, Pos, C.c_void_p, C.c_int32,
                                            C.c_void_p, C.c_void_p], C.c_int),
         "pfsf_debug_rcp64": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+        "pfsf_last_tick_report": ([E, C.POINTER(TickReport)], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
     }
@@ -278,6 +285,12 @@ class Engine:
     def island_report(self, iid):
         r = IslandReport()
         rc = self.L.pfsf_island_solve_report(self.h, iid, C.byref(r))
+        return rc, r
+
+    def tick_report(self):
+        """pfsf_last_tick_report: (rc, TickReport) of the last reference tick or tolerance-tick tail."""
+        r = TickReport()
+        rc = self.L.pfsf_last_tick_report(self.h, C.byref(r))
         return rc, r
 
     def read_solution64(self, iid, n):

@@ -184,7 +184,9 @@ def test_batched_tick_many_islands(eng):
         fb = np.zeros(1 + 4 * cap, np.int32)
         l0 = eng.launches()
         assert eng.tick_dbb(ids, fb) == capi.PFSF_OK
-        per_tick.append(eng.launches() - l0)
+        rc, rep = eng.tick_report()
+        assert rc == capi.PFSF_OK and rep.islands == len(ids) and rep.kernel_launches == eng.launches() - l0
+        per_tick.append((rep.groups, rep.kernel_launches, rep.graph_replayed))
         want = np.zeros(1 + 4 * cap, np.int32)
         for iid, host, ref, origin in isl:
             ref.tick()
@@ -193,8 +195,14 @@ def test_batched_tick_many_islands(eng):
         assert np.array_equal(fb[: 1 + 4 * fb[0]], want[: 1 + 4 * want[0]]), f"tick {t}: failure tuples"
         for iid, host, ref, origin in isl:
             _assert_island_state(eng, iid, host, ref, t)
-    # 24 islands one at a time would take ~24 x 200 launches per tick
-    assert max(per_tick) < 1500, per_tick
+    # one launch per schedule step and GROUP: at most one group per distinct
+    # (shape, schedule) here, and a schedule is at most ~700 launches (the
+    # aspect-8 rod: a V-cycle every step, twice); one island at a time the
+    # 24 islands would take at least 24 x 16 x 8 RBGS colour launches
+    for groups, launches, _ in per_tick:
+        assert groups <= 12 and launches <= 700 * groups and launches < 24 * 16 * 8, per_tick
+    # the structure repeats between some consecutive ticks: replayed graph
+    assert any(r for _, _, r in per_tick[1:]), per_tick
 
 
 def test_reference_fixtures_parity(eng):
