@@ -23,6 +23,15 @@ struct Engine::Arena {
     int persistent_ctas = 0;         // CTAs of the last batched launch(es)
     bool b_stale = false;            // b holds an adjoint right-hand side, not the sources
     double* xf = nullptr;            // adjoint: FP64 copy of the forward solution (own allocation)
+    KDesc* hdesc = nullptr;          // pinned host copy of the per-island results of the last solve
+    // the batched solve's launch sequence (queue reset, persistent launch(es),
+    // result copies) as a CUDA graph, captured on the second solve of this
+    // arena with the same parameters and replayed after
+    bool launched = false;
+    bool graph_off = false;          // capture failed once: launch directly from then on
+    cudaGraphExec_t solve_exec = nullptr;
+    std::vector<double> solve_key;
+    int graph_launches = 0, graph_ctas = 0;
 };
 
 }  // namespace pfsf_b200

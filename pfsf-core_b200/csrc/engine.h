@@ -200,7 +200,8 @@ private:
     void free_arena();
     bool collect_kappa_set(const int32_t* ids, int32_t count, std::vector<Island*>& set);
     KArena solve_params(double tol, int32_t max_iter) const;
-    pfsf_result run_solve(const KArena& k, std::vector<KDesc>& res, int64_t& launches);
+    pfsf_result run_solve(const KArena& k, int64_t& launches);
+    void collect_results(std::vector<KDesc>& res) const;
     bool grid_barrier_failed() const;
     void destroy_side();
     void fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_solve_stats& st) const;

@@ -1,6 +1,7 @@
 // Engine side of the tolerance solve: kappa-form registration, the packed
 // device arena for a set of islands, upload / solve / readback.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 
@@ -95,6 +96,8 @@ void Engine::free_arena() {
     if (!arena_) return;
     cudaStreamSynchronize(stream_);
     for (void* h : arena_->pinned) cudaHostUnregister(h);
+    if (arena_->solve_exec) cudaGraphExecDestroy(arena_->solve_exec);
+    if (arena_->hdesc) cudaFreeHost(arena_->hdesc);
     if (arena_->base) cudaFree(arena_->base);
     if (arena_->hscratch) cudaFreeHost(arena_->hscratch);
     if (arena_->xf) cudaFree(arena_->xf);
@@ -187,6 +190,7 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     k.nisl = nisl;
     k.prec = A->prec;
     if (!CU_OK(cudaMallocHost((void**)&A->hscratch, 256))) return false;
+    if (!CU_OK(cudaMallocHost((void**)&A->hdesc, sizeof(KDesc) * std::max(nisl, 1)))) return false;
     k.hscratch = A->hscratch;
     // largest island first (load balance of the persistent queue)
     std::vector<int> order(nisl);
@@ -253,38 +257,92 @@ KArena Engine::solve_params(double tol, int32_t max_iter) const {
 
 // Launches the solve of every island in the arena (x64 is the starting
 // guess, b the right-hand side) and queues the copy of the per-island
-// results into res (valid after the stream is synchronised).
-pfsf_result Engine::run_solve(const KArena& k, std::vector<KDesc>& res, int64_t& nl) {
+// results into the arena's pinned result records (collect_results reads
+// them after the stream is synchronised).
+pfsf_result Engine::run_solve(const KArena& k, int64_t& nl) {
     Arena& A = *arena_;
-    res.resize(A.desc.size());
+    const size_t nisl = A.desc.size();
     nl = 0;
-    if (solve_mode_ == PFSF_SOLVE_BATCHED) {
+    if (solve_mode_ != PFSF_SOLVE_BATCHED) {
+        for (size_t q = 0; q < nisl; q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &A.hdesc[q]);
+        launches_ += nl;
+        cudaMemcpyAsync(A.hdesc, k.desc, sizeof(KDesc) * nisl, cudaMemcpyDeviceToHost, stream_);
+        return PFSF_OK;
+    }
+    // islands at or above the grid threshold are solved by the whole GPU
+    // (one at a time), those at or above the cluster threshold by whole
+    // thread-block clusters (largest first), islands below the warp
+    // threshold by single warps, the rest by single CTAs
+    int ngiant = 0, nbig = 0, nsmall = 0;
+    for (const KDesc& d : A.desc) {
+        ngiant += d.n >= grid_min_voxels_ ? 1 : 0;
+        nbig += (d.n >= cluster_min_voxels_ && d.n < grid_min_voxels_) ? 1 : 0;
+        nsmall += d.n < warp_max_voxels_ ? 1 : 0;
+    }
+    int* flag = reinterpret_cast<int*>(A.hscratch) + 48;
+    auto enqueue = [&](int& launches) {
         cudaMemsetAsync(k.queue, 0, 16 * sizeof(int), stream_);
-        // islands at or above the grid threshold are solved by the whole GPU
-        // (one at a time), those at or above the cluster threshold by whole
-        // thread-block clusters (largest first), islands below the warp
-        // threshold by single warps, the rest by single CTAs
-        int ngiant = 0, nbig = 0, nsmall = 0;
-        for (const KDesc& d : A.desc) {
-            ngiant += d.n >= grid_min_voxels_ ? 1 : 0;
-            nbig += (d.n >= cluster_min_voxels_ && d.n < grid_min_voxels_) ? 1 : 0;
-            nsmall += d.n < warp_max_voxels_ ? 1 : 0;
-        }
-        int launches = 0;
         const int ctas = kappa::launch_batched(stream_, side_, k, ngiant, nbig, nsmall, cluster_size_, num_sms_,
                                                &launches);
-        if (ctas < 0) return PFSF_ERROR_VULKAN;
-        A.persistent_ctas = ctas;
-        nl = launches;
-        int* flag = reinterpret_cast<int*>(A.hscratch) + 48;
-        *flag = 0;
         cudaMemcpyAsync(flag, k.queue + 10, sizeof(int), cudaMemcpyDeviceToHost, stream_);
-    } else {
-        for (size_t q = 0; q < A.desc.size(); q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &res[q]);
+        cudaMemcpyAsync(A.hdesc, k.desc, sizeof(KDesc) * nisl, cudaMemcpyDeviceToHost, stream_);
+        return ctas;
+    };
+    // The whole-GPU tier's cooperative launch stays outside graphs; the rest
+    // is captured once the arena has run one direct solve (kernel attributes
+    // set, occupancy known) and replayed while the parameters stay the same.
+    const std::vector<double> key = {k.tol, k.eta_min, (double)k.max_inner, (double)k.max_outer, (double)k.omega_c,
+                                     (double)k.nu, (double)k.coarse_sweeps, (double)k.fp64_dots, (double)k.smoother,
+                                     (double)k.cheb_k, (double)k.prec, (double)nbig, (double)nsmall,
+                                     (double)cluster_size_, (double)num_sms_, (double)nisl};
+    *flag = 0;
+    if (ngiant == 0 && A.launched && !A.graph_off) {
+        if (A.solve_exec && A.solve_key != key) {
+            cudaGraphExecDestroy(A.solve_exec);
+            A.solve_exec = nullptr;
+        }
+        if (!A.solve_exec) {
+            cudaGraph_t graph = nullptr;
+            int launches = 0, ctas = -1;
+            if (CU_OK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed))) {
+                ctas = enqueue(launches);
+                const cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+                if (ce == cudaSuccess && graph && ctas >= 0 &&
+                    CU_OK(cudaGraphInstantiate(&A.solve_exec, graph, 0))) {
+                    A.solve_key = key;
+                    A.graph_launches = launches;
+                    A.graph_ctas = ctas;
+                } else {
+                    A.solve_exec = nullptr;
+                }
+                if (graph) cudaGraphDestroy(graph);
+            }
+            if (!A.solve_exec) {
+                std::fprintf(stderr, "[libpfsf] batched solve capture failed (%s); launching directly\n",
+                             cudaGetErrorString(cudaGetLastError()));
+                A.graph_off = true;
+            }
+        }
+        if (A.solve_exec) {
+            if (!CU_OK(cudaGraphLaunch(A.solve_exec, stream_))) return PFSF_ERROR_VULKAN;
+            A.persistent_ctas = A.graph_ctas;
+            nl = A.graph_launches;
+            launches_ += nl;
+            return PFSF_OK;
+        }
     }
+    int launches = 0;
+    const int ctas = enqueue(launches);
+    if (ctas < 0) return PFSF_ERROR_VULKAN;
+    A.persistent_ctas = ctas;
+    A.launched = true;
+    nl = launches;
     launches_ += nl;
-    cudaMemcpyAsync(res.data(), k.desc, sizeof(KDesc) * res.size(), cudaMemcpyDeviceToHost, stream_);
     return PFSF_OK;
+}
+
+void Engine::collect_results(std::vector<KDesc>& res) const {
+    res.assign(arena_->hdesc, arena_->hdesc + arena_->desc.size());
 }
 
 // After the stream is synchronised: did a whole-GPU barrier time out?
@@ -373,7 +431,7 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     if (flags & PFSF_SOLVE_COLD_START) cudaMemsetAsync(k.x64, 0, (size_t)A.nfine * 8, stream_);
     std::vector<KDesc> res;
     int64_t nl = 0;
-    if (pfsf_result rc = run_solve(k, res, nl); rc != PFSF_OK) return rc;
+    if (pfsf_result rc = run_solve(k, nl); rc != PFSF_OK) return rc;
     cudaEventRecord(ev[2], stream_);
     if (!(flags & PFSF_SOLVE_NO_READBACK)) {
         kappa::launch_to_f32(stream_, k, A.nfine);
@@ -388,6 +446,7 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     }
     cudaEventRecord(ev[3], stream_);
     if (!CU_OK(cudaStreamSynchronize(stream_)) || grid_barrier_failed()) return PFSF_ERROR_VULKAN;
+    collect_results(res);
     float t_up = 0, t_solve = 0, t_rb = 0;
     cudaEventElapsedTime(&t_up, ev[0], ev[1]);
     cudaEventElapsedTime(&t_solve, ev[1], ev[2]);
@@ -461,7 +520,7 @@ pfsf_result Engine::adjoint_to_tolerance(const int32_t* ids, int32_t count, doub
     cudaEventRecord(ev[1], stream_);
     std::vector<KDesc> res;
     int64_t nl = 0;
-    if (pfsf_result rc = run_solve(k, res, nl); rc != PFSF_OK) return rc;
+    if (pfsf_result rc = run_solve(k, nl); rc != PFSF_OK) return rc;
     // gradients into the (now free) r / z work vectors, then restore x64
     kappa::launch_edge_product(stream_, k, A.xf, A.nfine, k.r, k.z, num_sms_);
     launches_++;
@@ -480,6 +539,7 @@ pfsf_result Engine::adjoint_to_tolerance(const int32_t* ids, int32_t count, doub
     ok &= CU_OK(cudaMemcpyAsync(k.x64, A.xf, (size_t)A.nfine * 8, cudaMemcpyDeviceToDevice, stream_));
     cudaEventRecord(ev[3], stream_);
     if (!ok || !CU_OK(cudaStreamSynchronize(stream_)) || grid_barrier_failed()) return PFSF_ERROR_VULKAN;
+    collect_results(res);
     float t_up = 0, t_solve = 0, t_rb = 0;
     cudaEventElapsedTime(&t_up, ev[0], ev[1]);
     cudaEventElapsedTime(&t_solve, ev[1], ev[2]);
