@@ -155,6 +155,13 @@ typedef struct pfsf_tick_report {
 
 PFSF_API pfsf_result pfsf_last_tick_report(pfsf_engine engine, pfsf_tick_report* out);
 
+/* No counterpart in the reference's native ABI; the Java path reduces it on
+ * the GPU with phi_reduce_max.comp.glsl and feeds PFSFScheduler.checkDivergence.
+ * Largest phi of the island at the end of its last tick (reference or
+ * tolerance tick), reduced on the device in the same pass as the failure
+ * scan; 0 before the island's first tick. */
+PFSF_API pfsf_result pfsf_island_phi_max(pfsf_engine engine, int32_t island_id, float* out);
+
 /* Copies the FP64 solution accumulator of the last tolerance solve of an
  * island (count = min(N, capacity) values).  The FP32 phi written back by
  * pfsf_solve_to_tolerance is this vector rounded to float32. */

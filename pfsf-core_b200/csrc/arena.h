@@ -16,7 +16,7 @@ struct Engine::Arena {
     void* base = nullptr;            // single device allocation
     size_t bytes = 0;
     KArena dev{};                    // device pointers (into base)
-    float* hscratch = nullptr;       // pinned host scalars (plain mode)
+    float* hscratch = nullptr;       // pinned host words (the whole-GPU tier's barrier error flag)
     float* phi_out = nullptr;        // FP32 solution staging (device), aliases e
     std::vector<void*> pinned;       // host ranges registered for fast copies
     bool solved = false;             // x64 holds a forward solution of this island set
@@ -32,6 +32,7 @@ struct Engine::Arena {
     cudaGraphExec_t solve_exec = nullptr;
     std::vector<double> solve_key;
     int graph_launches = 0, graph_ctas = 0;
+    kappa::PlainGraphs plain;        // per-island graphs of the plain solve
 };
 
 }  // namespace pfsf_b200

@@ -33,7 +33,8 @@ struct CIsl {
     uint32_t* macro;
     float* res_macro;      // tick result: max macro residual
     int32_t* res_fail;     // tick result: failed voxels
-    int32_t *fcounts, *foffsets, *tuples;
+    uint32_t* res_phimax;  // tick result: max phi (order-preserving key)
+    int32_t *fcounts, *foffsets, *tuples;  // failed voxels per 256-voxel block, their offsets, tuples
     int32_t tuple_cap;
     int32_t iter0;         // chebyshev_iter at the start of the tick
     int32_t cur1, cur2;    // coarse ping-pong slots at the start of the tick
@@ -52,8 +53,8 @@ struct CIsl {
 };
 
 // Block-count kinds of a batched launch: grid voxels, the voxels of each of
-// the 8 colours, the two coarse levels, macro blocks, compaction chunks.
-enum BKind : int { kbN = 0, kbC0 = 1, kbN1 = 9, kbN2 = 10, kbMB = 11, kbFC = 12, kbKinds = 13 };
+// the 8 colours, the two coarse levels, macro blocks.
+enum BKind : int { kbN = 0, kbC0 = 1, kbN1 = 9, kbN2 = 10, kbMB = 11, kbKinds = 12 };
 
 // One island group as the launchers see it.
 struct BGroup {
@@ -88,8 +89,9 @@ void copy_damage(cudaStream_t s, const BGroup& g);
 void phase_field(cudaStream_t s, const BGroup& g, float l0, float gc, float relax, int split);
 void history(cudaStream_t s, const BGroup& g);
 void take_phi(cudaStream_t s, const BGroup& g);
+// failure codes, macro residual and phi maxima, failed-voxel block counts
 void failure_scan(cudaStream_t s, const BGroup& g);
-void macro_max(cudaStream_t s, const BGroup& g);
+// scan of the block counts and the tuple write (after failure_scan)
 void fail_compact(cudaStream_t s, const BGroup& g);
 void stress_out(cudaStream_t s, const BGroup& g);
 }  // namespace batch

@@ -632,24 +632,26 @@ __device__ __forceinline__ void d_phase_field(int lx, int ly, int lz, const floa
 
 // ---------------------------------------------------------------- failure scan
 // SH/failure_scan.comp.glsl:36-196
-__device__ __forceinline__ void d_failure_scan(int lx, int ly, int lz, const float* __restrict__ phi,
-                                                         const float* __restrict__ sigma,
-                                                         const float* __restrict__ rcomp,
-                                                         const uint8_t* __restrict__ type,
-                                                         uint8_t* __restrict__ fail,
-                                                         const float* __restrict__ rtens,
-                                                         uint32_t* __restrict__ macro,
-                                                         const float* __restrict__ rho, float phi_orphan, int64_t gt_, int64_t blk_) {
+// Failure code of voxel i (SH/failure_scan.comp.glsl:36-196): 0 intact, 2
+// crushing (compressive inflow above rcomp), 3 no support (no live face or
+// phi above the orphan level), 4 tension (outflow above rtens); air and
+// anchors 0.  For an intact solid voxel also its residual |fin - fout + rho|
+// (res, else -1) and its macro block (mb), which the reference feeds into
+// the macro-residual maximum.
+__device__ __forceinline__ uint8_t d_fail_code(int lx, int ly, int lz, const float* __restrict__ phi,
+                                               const float* __restrict__ sigma, const float* __restrict__ rcomp,
+                                               const uint8_t* __restrict__ type, const float* __restrict__ rtens,
+                                               const float* __restrict__ rho, float phi_orphan, int64_t i,
+                                               float& res, int64_t& mb) {
     const int64_t n = (int64_t)lx * ly * lz;
-    const int64_t i = gt_;
-    if (i >= n) return;
-    uint8_t code = 0;
-    if (type[i] != kSolid) { fail[i] = 0; return; }
+    res = -1.0f;
+    mb = 0;
+    if (type[i] != kSolid) return 0;
     const float p = phi[i];
     float s6[6];
     load_s6(sigma, n, i, s6);
     const float sum6 = s6[0] + s6[1] + s6[2] + s6[3] + s6[4] + s6[5];
-    if (sum6 == 0.0f || p > phi_orphan) { fail[i] = 3; return; }
+    if (sum6 == 0.0f || p > phi_orphan) return 3;
     const int x = (int)(i % lx);
     const int64_t rem = i / lx;
     const int y = (int)(rem % ly), z = (int)(rem / ly);
@@ -691,14 +693,36 @@ __device__ __forceinline__ void d_failure_scan(int lx, int ly, int lz, const flo
         }
     }
     const float rc = rcomp[i], rt = rtens[i];
-    if (rc > 0.0f && fin > rc) code = 2;
-    else if (rt > 0.0f && fout > rt) code = 4;
-    fail[i] = code;
-    if (code != 0) return;
-    const float res = fabsf(fin - fout + rho[i]);
+    if (rc > 0.0f && fin > rc) return 2;
+    if (rt > 0.0f && fout > rt) return 4;
+    res = fabsf(fin - fout + rho[i]);
     const int mbx = (lx + kMacroBlock - 1) / kMacroBlock, mby = (ly + kMacroBlock - 1) / kMacroBlock;
-    const int64_t mb = (x / kMacroBlock) + (int64_t)mbx * ((y / kMacroBlock) + (int64_t)mby * (z / kMacroBlock));
-    atomicMax(macro + mb, __float_as_uint(res));
+    mb = (x / kMacroBlock) + (int64_t)mbx * ((y / kMacroBlock) + (int64_t)mby * (z / kMacroBlock));
+    return 0;
+}
+
+// Order-preserving map of a float onto uint32 (atomicMax over keys = max over
+// floats, negatives included); 0 is below every key.
+__device__ __forceinline__ uint32_t float_key(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// Block-wide max (valid in thread 0).
+__device__ __forceinline__ float block_max(float v) {
+    __shared__ float warp_part[kBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) warp_part[w] = v;
+    __syncthreads();
+    float m = -INFINITY;
+    if (w == 0) {
+        m = lane < (kBlock / 32) ? warp_part[lane] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    }
+    return m;
 }
 
 __device__ __forceinline__ void d_macro_fill(uint32_t* __restrict__ macro, int64_t nmb, int64_t gt_, int64_t blk_) {
@@ -708,22 +732,6 @@ __device__ __forceinline__ void d_macro_fill(uint32_t* __restrict__ macro, int64
 
 // max over macro blocks as float (readbackMacroResidualMax, island_buffer.cpp:1012-1090),
 // single block; writes out[0].
-__device__ __forceinline__ void d_macro_max(const uint32_t* __restrict__ macro, int64_t nmb,
-                                                      float* __restrict__ out, int64_t gt_, int64_t blk_) {
-    __shared__ float warp_part[kBlock / 32];
-    float m = 0.0f;
-    for (int64_t k = threadIdx.x; k < nmb; k += kBlock) m = fmaxf(m, __uint_as_float(macro[k]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        float s = threadIdx.x < kBlock / 32 ? warp_part[threadIdx.x] : 0.0f;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_down_sync(0xffffffffu, s, o));
-        if (threadIdx.x == 0) out[0] = s;
-    }
-}
 
 // ---------------------------------------------------------------- failure compaction
 constexpr int kCompactChunk = 4096;  // voxels per block
@@ -892,6 +900,10 @@ __global__ void __launch_bounds__(kBlock) kb_macro_fill(const CIsl* __restrict__
                                                         int nisl) {
     BATCH_ISLAND
     d_macro_fill(I.macro, I.nmb, t_, lb_);
+    if (t_ == 0) {  // the island records the failure pass reduces into
+        *I.res_macro = __uint_as_float(kMacroSeedBits);
+        *I.res_phimax = 0u;
+    }
 }
 __global__ void __launch_bounds__(kBlock) kb_rbgs_color(const CIsl* __restrict__ tab, const int* __restrict__ bs,
                                                         int nisl, int color, int sidx, int warm, float dampf) {
@@ -985,32 +997,62 @@ __global__ void __launch_bounds__(kBlock) kb_history(const CIsl* __restrict__ ta
     BATCH_ISLAND
     d_history(I.lx, I.ly, I.lz, I.phi, I.sigma, I.type, I.H, t_);
 }
+// One pass over the voxels after the phase field: failure code, macro
+// residual (per macro block and the island's maximum, the readback of
+// island_buffer.cpp:968-1090), the island's phi maximum (SH/phi_reduce_max.comp.glsl,
+// the divergence check's input) and the failed voxels of each 256-voxel
+// block (the counts the compaction scans).  NaN residuals and NaN phi do not
+// enter the island maxima.
 __global__ void __launch_bounds__(kBlock) kb_failure_scan(const CIsl* __restrict__ tab, const int* __restrict__ bs,
                                                           int nisl) {
     BATCH_ISLAND
-    d_failure_scan(I.lx, I.ly, I.lz, I.phi, I.sigma, I.rcomp, I.type, I.fail, I.rtens, I.macro, I.src, kPhiOrphan,
-                   t_, lb_);
+    float res = -1.0f, ph = -INFINITY;
+    uint8_t code = 0;
+    if (t_ < I.n) {
+        int64_t mb = 0;
+        code = d_fail_code(I.lx, I.ly, I.lz, I.phi, I.sigma, I.rcomp, I.type, I.rtens, I.src, kPhiOrphan, t_, res, mb);
+        I.fail[t_] = code;
+        if (res >= 0.0f || isnan(res)) atomicMax(I.macro + mb, __float_as_uint(res));
+        ph = I.phi[t_];
+        if (isnan(ph)) ph = -INFINITY;
+        if (isnan(res)) res = -1.0f;
+    }
+    const int failed = __syncthreads_count(code != 0);
+    const float mres = block_max(res);
+    __syncthreads();
+    const float mphi = block_max(ph);
+    if (threadIdx.x == 0) {
+        I.fcounts[lb_] = failed;
+        if (mres >= 0.0f) atomicMax(reinterpret_cast<uint32_t*>(I.res_macro), __float_as_uint(mres));
+        if (mphi > -INFINITY) atomicMax(I.res_phimax, float_key(mphi));
+    }
 }
-// one block per island
-__global__ void __launch_bounds__(kBlock) kb_macro_max(const CIsl* __restrict__ tab) {
-    const CIsl& I = tab[blockIdx.x];
-    d_macro_max(I.macro, I.nmb, I.res_macro, 0, 0);
-}
-__global__ void __launch_bounds__(kBlock) kb_fail_count(const CIsl* __restrict__ tab, const int* __restrict__ bs,
-                                                        int nisl) {
-    BATCH_ISLAND
-    d_fail_count(I.fail, I.n, I.fcounts, t_, lb_);
-}
-// one block per island
+// one block per island: exclusive scan of the 256-voxel block counts
 __global__ void __launch_bounds__(kBlock) kb_fail_scan(const CIsl* __restrict__ tab) {
     const CIsl& I = tab[blockIdx.x];
-    d_fail_scan(I.fcounts, ceil_div64(I.n, kCompactChunk), I.foffsets, I.res_fail, 0, 0);
+    d_fail_scan(I.fcounts, ceil_div64(I.n, kBlock), I.foffsets, I.res_fail, 0, 0);
 }
+// {x, y, z, code} tuples of one 256-voxel block at its scanned offset, in
+// voxel order; tuples at or beyond the island's capacity are dropped.
 __global__ void __launch_bounds__(kBlock) kb_fail_write(const CIsl* __restrict__ tab, const int* __restrict__ bs,
                                                         int nisl) {
     BATCH_ISLAND
-    d_fail_write(I.fail, I.lx, I.ly, I.lz, I.ox, I.oy, I.oz, I.foffsets, I.tuples, I.tuples ? I.tuple_cap : 0, t_,
-                 lb_);
+    __shared__ int32_t warp_cnt[kBlock / 32];
+    const uint8_t f = t_ < I.n ? I.fail[t_] : 0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, f != 0);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) warp_cnt[w] = __popc(ballot);
+    __syncthreads();
+    int before = 0;
+    for (int q = 0; q < w; q++) before += warp_cnt[q];
+    const int64_t pos = (int64_t)I.foffsets[lb_] + before + __popc(ballot & ((1u << lane) - 1u));
+    if (f != 0 && I.tuples && pos < I.tuple_cap) {
+        int32_t* t = I.tuples + 4 * pos;
+        t[0] = I.ox + (int)(t_ % I.lx);
+        t[1] = I.oy + (int)((t_ / I.lx) % I.ly);
+        t[2] = I.oz + (int)(t_ / ((int64_t)I.lx * I.ly));
+        t[3] = f;
+    }
 }
 // phi into the caller's stress readback buffer (device-visible host memory)
 __global__ void __launch_bounds__(kBlock) kb_stress_out(const CIsl* __restrict__ tab, const int* __restrict__ bs,
@@ -1050,7 +1092,6 @@ int64_t batch_blocks(const CIsl& I, int kind) {
     if (kind == kbN1) return ceil_div64(I.n1, kBlock);
     if (kind == kbN2) return ceil_div64(I.n2, kBlock);
     if (kind == kbMB) return ceil_div64(I.nmb, kBlock);
-    if (kind == kbFC) return ceil_div64(I.n, kCompactChunk);
     return 0;
 }
 
@@ -1093,13 +1134,9 @@ void phase_field(cudaStream_t s, const BGroup& g, float l0, float gc, float rela
 void history(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_history); }
 void take_phi(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_take_phi); }
 void failure_scan(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_failure_scan); }
-void macro_max(cudaStream_t s, const BGroup& g) {
-    if (g.nisl > 0) kb_macro_max<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab);
-}
 void fail_compact(cudaStream_t s, const BGroup& g) {
-    BLAUNCH(kbFC, kb_fail_count);
     if (g.nisl > 0) kb_fail_scan<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab);
-    BLAUNCH(kbFC, kb_fail_write);
+    BLAUNCH(kbN, kb_fail_write);
 }
 void stress_out(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_stress_out); }
 #undef BLAUNCH

@@ -193,7 +193,7 @@ bool Engine::ensure_compat(Island& s) {
     s.type = (uint8_t*)dalloc(s, (size_t)n); ok &= s.type != nullptr;
     s.fail = (uint8_t*)dalloc(s, (size_t)n); ok &= s.fail != nullptr;
     s.macro = (uint32_t*)dalloc(s, (size_t)std::max<int64_t>(s.nmb, 1) * 4); ok &= s.macro != nullptr;
-    const int64_t nb = compat::fail_compact_blocks(n);
+    const int64_t nb = compat::pcg_blocks(n);  // failed voxels per 256-voxel block
     s.fcounts = (int32_t*)dalloc(s, (size_t)nb * 4); ok &= s.fcounts != nullptr;
     s.foffsets = (int32_t*)dalloc(s, (size_t)nb * 4); ok &= s.foffsets != nullptr;
     if (!ok) {
@@ -446,6 +446,11 @@ pfsf_result Engine::finish_dispatch(const std::vector<Island*>& dispatched, bool
             Island* s = dispatched[k];
             s->prev_macro = s->last_macro;
             s->last_macro = host_results_[k].macro_max;
+            const uint32_t key = host_results_[k].phi_max_key;
+            if (key != 0u) {
+                const uint32_t b = (key & 0x80000000u) ? (key & 0x7fffffffu) : ~key;
+                std::memcpy(&s->phi_max, &b, 4);
+            }
             const int32_t total = host_results_[k].fail_total;
             if (drain && total > 0 && dbb_count < dbb_cap) {
                 const int32_t take = std::min(total, dbb_cap - dbb_count);
@@ -467,6 +472,14 @@ pfsf_result Engine::finish_dispatch(const std::vector<Island*>& dispatched, bool
         if (drain) *static_cast<int32_t*>(fail_addr) = dbb_count;
         if (result) result->count = legacy_count;
     }
+    return PFSF_OK;
+}
+
+pfsf_result Engine::island_phi_max(int32_t id, float* out) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    Island* s = find(id);
+    if (!out || !s) return PFSF_ERROR_INVALID_ARG;
+    *out = s->phi_max;
     return PFSF_OK;
 }
 

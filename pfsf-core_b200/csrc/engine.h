@@ -72,7 +72,8 @@ struct HostBuffers {
 struct TickResult {
     float macro_max;
     int32_t fail_total;
-    int32_t pad[2];
+    uint32_t phi_max_key;  // order-preserving key of the max phi (0: none)
+    int32_t pad;
 };
 
 struct KappaState;  // tolerance-solve state (kappa_solver.cu)
@@ -111,6 +112,9 @@ struct Island {
     // sparse upload region (pinned host) + device staging
     void* sparse_host = nullptr;
     void* sparse_dev = nullptr;
+
+    // max phi at the end of the last tick (the divergence check's input)
+    float phi_max = 0.0f;
 
     // schedule state
     int chebyshev_iter = 0;
@@ -170,6 +174,7 @@ public:
                                      uint32_t flags, pfsf_solve_stats* out);
     pfsf_result debug_read_field(int32_t id, int32_t field, void* out, int64_t bytes, int64_t* out_bytes);
     pfsf_result last_tick_report(pfsf_tick_report* out) const;
+    pfsf_result island_phi_max(int32_t id, float* out);
 
     cudaStream_t stream() const { return stream_; }
     int num_sms() const { return num_sms_; }

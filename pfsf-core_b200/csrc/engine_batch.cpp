@@ -71,8 +71,8 @@ double tick_bytes(const Island& s, const Plan& p, bool tail_only, bool phase, bo
         if (p.pcg) b += (28.0 + 33.0 + 41.0) * n + p.pc * (33.0 + 53.0 + 37.0) * n;
     }
     if (phase) b += 8.0 * n + 47.0 * n;
-    b += 42.0 * n;               // failure scan
-    if (compact) b += 2.0 * n;   // compaction reads the flags twice
+    b += 42.0 * n;               // failure pass (codes, residual and phi maxima, block counts)
+    if (compact) b += 1.0 * n;   // the tuple write reads the codes once
     if (uploaded) b += 45.0 * n; // the uploaded arrays written into HBM
     if (stress) b += 4.0 * n;    // phi read for the stress readback
     return b;
@@ -229,6 +229,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
         c.hyd = s.hyd; c.H = s.H; c.D = s.D; c.Dold = s.Dold; c.type = s.type; c.fail = s.fail; c.macro = s.macro;
         c.res_macro = &B.d_res[k].macro_max;
         c.res_fail = &B.d_res[k].fail_total;
+        c.res_phimax = &B.d_res[k].phi_max_key;
         c.fcounts = s.fcounts; c.foffsets = s.foffsets;
         c.tuples = want_cap > 0 ? s.tuples : nullptr;
         c.tuple_cap = (int32_t)std::min<int64_t>(want_cap, s.n);
@@ -421,11 +422,10 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
             nl += 2;
         }
         compat::batch::failure_scan(st, ALL);
-        compat::batch::macro_max(st, ALL);
-        nl += 2;
+        nl++;
         if (want_cap > 0) {
             compat::batch::fail_compact(st, ALL);
-            nl += 3;
+            nl += 2;
         }
         compat::batch::stress_out(st, ALL);
         nl++;

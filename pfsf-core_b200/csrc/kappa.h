@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace pfsf_b200 {
 
 // Levels of the hierarchy (fine + 4 coarse).  Measured with 8 (coarsest
@@ -85,8 +87,7 @@ struct KArena {
     int nu;                // pre/post smoothing sweeps
     int coarse_sweeps;     // symmetric sweeps on the coarsest level
     int fp64_dots;         // inner products in FP64 (1) or FP32 (0)
-    float* scratch;        // plain mode: block partials + scalars (device)
-    float* hscratch;       // plain mode: pinned host scalars
+    float* scratch;        // block partials + the plain solve's control record (device)
     // Chebyshev smoother (smoother == 1): fine-level inverse diagonal and
     // update vectors, coarse update vector, per-step coefficients
     float* dinv0;
@@ -130,9 +131,18 @@ int launch_batched(cudaStream_t s, const SideStream& side, const KArena& a, int 
                    int cluster, int num_sms, int* launches);
 // Prepare kernels: sanitise kappa, round to 16-bit, zero non-solid source.
 void launch_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total, const int64_t* dummy);
-// Per-island plain solve driven from the host (one kernel per operation).
-// Returns kernel launches issued; writes results into desc (device) and hres (host copy).
-int64_t solve_plain(cudaStream_t s, const KArena& a, int isl, const KDesc& hdesc, KDesc* hres);
+// Per-island CUDA graphs of the plain solve, kept with the arena.
+struct PlainGraphs {
+    std::vector<cudaGraphExec_t> exec;  // per island (nullptr: not built yet)
+    std::vector<double> key;            // solve parameters the graphs were built for
+    cudaStream_t aux[2] = {nullptr, nullptr};  // capture streams of the loop bodies
+};
+void free_plain_graphs(PlainGraphs& g);
+// Per-island plain solve (one grid-wide kernel per operation, loops on the
+// device): launches the island's graph, building it on first use.  Writes
+// the results into desc (device).  Returns the graph launches issued, 0 if
+// the graph could not be built or launched.
+int64_t solve_plain(cudaStream_t s, const KArena& a, int isl, const KDesc& hdesc, PlainGraphs& cache);
 int batched_threads();
 int64_t plain_scratch_floats();
 // Adjoint: b = g on solid voxels, x64 = 0 (kappa_adjoint.cu).

@@ -97,6 +97,7 @@ void Engine::free_arena() {
     cudaStreamSynchronize(stream_);
     for (void* h : arena_->pinned) cudaHostUnregister(h);
     if (arena_->solve_exec) cudaGraphExecDestroy(arena_->solve_exec);
+    kappa::free_plain_graphs(arena_->plain);
     if (arena_->hdesc) cudaFreeHost(arena_->hdesc);
     if (arena_->base) cudaFree(arena_->base);
     if (arena_->hscratch) cudaFreeHost(arena_->hscratch);
@@ -191,7 +192,6 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     k.prec = A->prec;
     if (!CU_OK(cudaMallocHost((void**)&A->hscratch, 256))) return false;
     if (!CU_OK(cudaMallocHost((void**)&A->hdesc, sizeof(KDesc) * std::max(nisl, 1)))) return false;
-    k.hscratch = A->hscratch;
     // largest island first (load balance of the persistent queue)
     std::vector<int> order(nisl);
     std::iota(order.begin(), order.end(), 0);
@@ -264,7 +264,11 @@ pfsf_result Engine::run_solve(const KArena& k, int64_t& nl) {
     const size_t nisl = A.desc.size();
     nl = 0;
     if (solve_mode_ != PFSF_SOLVE_BATCHED) {
-        for (size_t q = 0; q < nisl; q++) nl += kappa::solve_plain(stream_, k, (int)q, A.desc[q], &A.hdesc[q]);
+        for (size_t q = 0; q < nisl; q++) {
+            const int64_t l = kappa::solve_plain(stream_, k, (int)q, A.desc[q], A.plain);
+            if (l <= 0) return PFSF_ERROR_VULKAN;
+            nl += l;
+        }
         launches_ += nl;
         cudaMemcpyAsync(A.hdesc, k.desc, sizeof(KDesc) * nisl, cudaMemcpyDeviceToHost, stream_);
         return PFSF_OK;

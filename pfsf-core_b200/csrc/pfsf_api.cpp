@@ -181,6 +181,11 @@ PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine e, int32_t id, pfsf_is
     return g ? g->island_report(id, out) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_island_phi_max(pfsf_engine e, int32_t id, float* out) {
+    Engine* g = E(e);
+    return g ? g->island_phi_max(id, out) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_last_tick_report(pfsf_engine e, pfsf_tick_report* out) {
     Engine* g = E(e);
     return g ? g->last_tick_report(out) : PFSF_ERROR_INVALID_ARG;

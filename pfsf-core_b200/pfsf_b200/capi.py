@@ -161,6 +161,7 @@ def load():
                                            C.c_void_p, C.c_void_p], C.c_int),
         "pfsf_debug_rcp64": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
         "pfsf_last_tick_report": ([E, C.POINTER(TickReport)], C.c_int),
+        "pfsf_island_phi_max": ([E, C.c_int32, C.POINTER(C.c_float)], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
     }
@@ -292,6 +293,12 @@ class Engine:
         r = TickReport()
         rc = self.L.pfsf_last_tick_report(self.h, C.byref(r))
         return rc, r
+
+    def phi_max(self, iid):
+        """pfsf_island_phi_max: (rc, max phi of the island's last tick)."""
+        v = C.c_float(0.0)
+        rc = self.L.pfsf_island_phi_max(self.h, iid, C.byref(v))
+        return rc, v.value
 
     def read_solution64(self, iid, n):
         out = np.zeros(n, np.float64)

@@ -70,6 +70,9 @@ def _assert_island_state(eng, iid, host, ref, t):
     err = float(np.abs(host["phi"].astype(np.float64) - phi_ref).max()) / scale
     assert err <= PHI_TOL, f"tick {t}: phi rel err {err:.3e}"
     assert np.array_equal(eng.debug_field(iid, 3), ref.view("fail").astype(np.uint8)), f"tick {t}: fail flags"
+    # the island's phi maximum, reduced in the failure pass
+    rc, pm = eng.phi_max(iid)
+    assert rc == capi.PFSF_OK and pm == float(eng.debug_field(iid, 0).max()), f"tick {t}: phi max"
     for field, name in ((1, "H"), (2, "D")):
         g = eng.debug_field(iid, field)
         r = ref.view(name)
