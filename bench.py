@@ -363,6 +363,7 @@ def run_ours(args):
         torch.cuda.synchronize()
     launches = eng.launches() - launches0
     ms = ev0.elapsed_time(ev1) / args.steps
+    tuning = eng.tuning()[1].as_dict()  # launch shapes (tuning file / environment / defaults)
     if args.island_report and rank == 0:
         write_island_report(args.island_report, eng, ids, isls)
     if ws > 1:
@@ -495,10 +496,8 @@ def run_ours(args):
                                            "coarse": stats[-1].vcycle_coarse_ms_sum,
                                            "tail": stats[-1].vcycle_tail_ms_sum},
                          "persistent_ctas": stats[-1].persistent_ctas,
-                         "cluster": os.environ.get("PFSF_CLUSTER", "4"),
-                         "cluster_min_voxels": os.environ.get("PFSF_CLUSTER_MIN_VOXELS", "262144"),
-                         "warp_max_voxels": os.environ.get("PFSF_WARP_MAX_VOXELS", "0"),
-                         "smoother": os.environ.get("PFSF_SMOOTHER", "chebyshev(batched)"), "cheb_k": os.environ.get("PFSF_CHEB_K", "3")},
+                         "tuning": tuning,
+                         "smoother": os.environ.get("PFSF_SMOOTHER", "chebyshev(batched)")},
         }
         print(json.dumps(line), flush=True)
     eng.close()

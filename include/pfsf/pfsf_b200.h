@@ -134,6 +134,35 @@ typedef struct pfsf_island_report {
 
 PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine engine, int32_t island_id, pfsf_island_report* out);
 
+/* No counterpart in the reference ABI.  Launch-shape parameters of the
+ * batched tolerance solve.  pfsf_init takes them from the tuning file the
+ * autotuner writes (pfsf_b200/autotune.py: timed trials on a size-bucketed
+ * island set, one section per GPU model and SM count) -- the file named by
+ * PFSF_TUNE_FILE, else tune/pfsf_tune.txt beside the library's lib/
+ * directory -- then from the PFSF_CLUSTER, PFSF_CLUSTER_MIN_VOXELS,
+ * PFSF_GRID_MIN_VOXELS, PFSF_WARP_MAX_VOXELS, PFSF_CHEB_K variables when set;
+ * built-in defaults otherwise. */
+typedef enum pfsf_tuning_source {
+    PFSF_TUNING_DEFAULT = 0,  /* built-in defaults */
+    PFSF_TUNING_FILE = 1,     /* the tuning file's section for this GPU */
+    PFSF_TUNING_ENV = 2,      /* at least one environment override */
+    PFSF_TUNING_CALLER = 3    /* pfsf_set_tuning */
+} pfsf_tuning_source;
+
+typedef struct pfsf_tuning {
+    int32_t struct_bytes;
+    int32_t cluster;              /* CTAs per thread-block cluster for big islands: 1 (none), 4 or 8 */
+    int64_t cluster_min_voxels;   /* islands of at least this many voxels go to clusters */
+    int64_t grid_min_voxels;      /* ... to the whole GPU, one at a time */
+    int64_t warp_max_voxels;      /* islands below this many voxels go to single warps (0: none) */
+    int32_t cheb_k;               /* Chebyshev smoothing degree, 1..4 */
+    int32_t source;               /* pfsf_tuning_source (read only) */
+} pfsf_tuning;
+
+PFSF_API pfsf_result pfsf_get_tuning(pfsf_engine engine, pfsf_tuning* out);
+/* INVALID_ARG for out-of-range values (nothing changes then). */
+PFSF_API pfsf_result pfsf_set_tuning(pfsf_engine engine, const pfsf_tuning* in);
+
 /* No counterpart in the reference ABI.  Shape of the last reference tick
  * (pfsf_tick_dbb / pfsf_tick) or tolerance-tick tail: the dispatched islands
  * run as groups of equal schedule, each schedule step one kernel launch over

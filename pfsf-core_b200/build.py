@@ -11,6 +11,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -43,19 +44,32 @@ def sources():
     return out
 
 
-def headers_mtime():
-    m = 0.0
-    for d in (CSRC, os.path.join(INCLUDE, "pfsf")):
-        for f in os.listdir(d):
-            if f.endswith((".h", ".cuh")):
-                m = max(m, os.path.getmtime(os.path.join(d, f)))
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def dep_mtime(path, seen=None):
+    """Newest mtime of a source and of every project header it includes
+    (directly or through other project headers)."""
+    seen = set() if seen is None else seen
+    if path in seen:
+        return 0.0
+    seen.add(path)
+    m = os.path.getmtime(path)
+    with open(path, errors="replace") as f:
+        text = f.read()
+    for inc in _INCLUDE_RE.findall(text):
+        for d in (os.path.dirname(path), CSRC, INCLUDE):
+            cand = os.path.join(d, inc)
+            if os.path.exists(cand):
+                m = max(m, dep_mtime(cand, seen))
+                break
     return m
 
 
-def compile_one(src, force, hm):
+def compile_one(src, force):
     path = os.path.join(CSRC, src)
     obj = os.path.join(OBJ, src + ".o")
-    if not force and os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(path), hm):
+    if not force and os.path.exists(obj) and os.path.getmtime(obj) > dep_mtime(path):
         return obj, None
     if src.endswith(".cu"):
         cmd = [NVCC] + ARCH + NVCC_FLAGS + EXTRA.get(src, []) + ["-c", path, "-o", obj]
@@ -69,10 +83,9 @@ def compile_one(src, force, hm):
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    hm = headers_mtime()
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
-        results = list(ex.map(lambda s: compile_one(s, force, hm), srcs))
+        results = list(ex.map(lambda s: compile_one(s, force), srcs))
     errs = [e for _, e in results if e]
     if errs:
         raise RuntimeError("libpfsf build failed:\n" + "\n".join(errs))

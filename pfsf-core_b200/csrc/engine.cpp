@@ -30,12 +30,7 @@ Island::~Island() = default;
 
 Engine::Engine(const pfsf_config& cfg) : cfg_(cfg) {
     if (const char* f = std::getenv("PFSF_FAULT_ALLOC_AFTER")) fault_alloc_after_ = std::atoll(f);
-    if (const char* f = std::getenv("PFSF_CLUSTER_MIN_VOXELS")) cluster_min_voxels_ = std::atoll(f);
-    if (const char* f = std::getenv("PFSF_GRID_MIN_VOXELS")) grid_min_voxels_ = std::atoll(f);
-    if (const char* f = std::getenv("PFSF_CLUSTER")) cluster_size_ = std::atoi(f);
-    if (const char* f = std::getenv("PFSF_WARP_MAX_VOXELS")) warp_max_voxels_ = std::atoll(f);
     if (const char* f = std::getenv("PFSF_SMOOTHER")) smoother_ = std::atoi(f);
-    if (const char* f = std::getenv("PFSF_CHEB_K")) cheb_k_ = std::atoi(f);
 }
 
 Engine::~Engine() { shutdown(); }
@@ -54,6 +49,7 @@ pfsf_result Engine::init() {
     if (!CU_OK(cudaSetDevice(dev))) return PFSF_ERROR_NO_DEVICE;
     device_ = dev;
     cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev);
+    load_tuning();
     if (!CU_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) return PFSF_ERROR_VULKAN;
     // side stream of the batched solve (fills CTA slots clusters leave free);
     // without it the solve runs on stream_ alone

@@ -161,6 +161,8 @@ public:
     void set_wind(const pfsf_vec3* w) { wind_ = w ? *w : pfsf_vec3{0, 0, 0}; }
     void set_precision(pfsf_precision p) { precision_ = p; }
     void set_solve_mode(pfsf_solve_mode m) { solve_mode_ = m; }
+    pfsf_result get_tuning(pfsf_tuning* out) const;
+    pfsf_result set_tuning(const pfsf_tuning* in);
 
     pfsf_result register_kappa(int32_t id, const pfsf_island_kappa_buffers* b);
     pfsf_result solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter, uint32_t flags,
@@ -248,6 +250,8 @@ private:
     int64_t warp_max_voxels_ = 0;         // PFSF_WARP_MAX_VOXELS (0: no warp tier)
     int smoother_ = -1;                   // PFSF_SMOOTHER (-1: mode default)
     int cheb_k_ = 3;                      // PFSF_CHEB_K
+    int tuning_source_ = PFSF_TUNING_DEFAULT;
+    void load_tuning();                   // tuning file, then environment overrides (init)
 };
 
 }  // namespace pfsf_b200

@@ -181,6 +181,16 @@ PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine e, int32_t id, pfsf_is
     return g ? g->island_report(id, out) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_get_tuning(pfsf_engine e, pfsf_tuning* out) {
+    Engine* g = E(e);
+    return g ? g->get_tuning(out) : PFSF_ERROR_INVALID_ARG;
+}
+
+PFSF_API pfsf_result pfsf_set_tuning(pfsf_engine e, const pfsf_tuning* in) {
+    Engine* g = E(e);
+    return g ? g->set_tuning(in) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_island_phi_max(pfsf_engine e, int32_t id, float* out) {
     Engine* g = E(e);
     return g ? g->island_phi_max(id, out) : PFSF_ERROR_INVALID_ARG;

@@ -106,6 +106,18 @@ class TickReport(C.Structure):
                 ("grid_voxels", C.c_double), ("device_ms", C.c_float), ("reserved", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    SOURCES = {0: "default", 1: "file", 2: "env", 3: "caller"}
+    _fields_ = [("struct_bytes", C.c_int32), ("cluster", C.c_int32), ("cluster_min_voxels", C.c_int64),
+                ("grid_min_voxels", C.c_int64), ("warp_max_voxels", C.c_int64), ("cheb_k", C.c_int32),
+                ("source", C.c_int32)]
+
+    def as_dict(self):
+        return {"cluster": self.cluster, "cluster_min_voxels": self.cluster_min_voxels,
+                "grid_min_voxels": self.grid_min_voxels, "warp_max_voxels": self.warp_max_voxels,
+                "cheb_k": self.cheb_k, "source": self.SOURCES.get(self.source, str(self.source))}
+
+
 _lib = None
 
 
@@ -162,6 +174,8 @@ def load():
         "pfsf_debug_rcp64": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
         "pfsf_last_tick_report": ([E, C.POINTER(TickReport)], C.c_int),
         "pfsf_island_phi_max": ([E, C.c_int32, C.POINTER(C.c_float)], C.c_int),
+        "pfsf_get_tuning": ([E, C.POINTER(Tuning)], C.c_int),
+        "pfsf_set_tuning": ([E, C.POINTER(Tuning)], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
     }
@@ -293,6 +307,19 @@ class Engine:
         r = TickReport()
         rc = self.L.pfsf_last_tick_report(self.h, C.byref(r))
         return rc, r
+
+    def tuning(self):
+        t = Tuning()
+        rc = self.L.pfsf_get_tuning(self.h, C.byref(t))
+        return rc, t
+
+    def set_tuning(self, **kw):
+        """pfsf_set_tuning with the current values updated by kw."""
+        rc, t = self.tuning()
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        t.struct_bytes = C.sizeof(Tuning)
+        return self.L.pfsf_set_tuning(self.h, C.byref(t))
 
     def phi_max(self, iid):
         """pfsf_island_phi_max: (rc, max phi of the island's last tick)."""
