@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["batch", "single", "adjoint", "fracture", "tick_dbb"], default="batch")
     ap.add_argument("--ticks", type=int, default=200, help="fracture workload: ticks")
-    ap.add_argument("--fd-voxels", type=int, default=256)
+    ap.add_argument("--fd-voxels", type=int, default=32)
     ap.add_argument("--dims", default="256,256,128", help="single workload: island sides x,y,z")
     ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
                     help="batch workload with N GPUs: every rank its own 4096 islands (weak) or one 4096-island "
@@ -506,76 +506,94 @@ def run_ours(args):
 
 
 def run_adjoint(args):
-    """Calibration gradient on one 128x128x64 noise island: 32 ticks with the
-    load ramped linearly to 2x (checkpoint every 8 ticks), loss
-    L = sum softplus(flux_in / rcomp - 1) + 1/2 ||phi - phi_target||^2 at the
-    last tick (rcomp in Pa: flux in N over a 1 m^2 face), phi_target = the
-    solution for kappa perturbed by a seeded lognormal (sigma 0.2) factor.
-    Reports ms per forward tick, ms of the backward (adjoint solve + edge
-    product), and the adjoint gradient's error against central finite
-    differences (h = 2^-10 on kappa) at --fd-voxels random voxels."""
+    """Calibration gradient over a trajectory: one 128x128x64 noise island,
+    32 ticks with the load ramped linearly to 2x (checkpoint every 8 ticks),
+    L = sum over ticks of [sum softplus(flux_in / rcomp - 1) + 1/2 ||phi_t -
+    f_t phi_target||^2] + sum softplus(H / h_scale - 1) with H = max over
+    ticks of psi_e (Amor split, the history update's formula) --
+    pfsf_b200.adjoint.trajectory_loss; rcomp in Pa (flux in N over a 1 m^2
+    face), phi_target = the solution for kappa perturbed by a seeded lognormal
+    (sigma 0.2) factor, h_scale = half the largest psi_e of the last tick.
+    Backward: every tick's device adjoint in reverse order, every tick but the
+    last re-solved from its checkpoint first.  Reports ms per forward tick,
+    the backward, the gradient's error against central differences
+    (h = 2^-10 on kappa, --fd-voxels voxels, the whole trajectory re-evaluated
+    per step) and, on a reduced 32x32x16 island over 8 ticks, against the
+    oracle's FP64 trajectory gradient."""
     os.environ.setdefault("PFSF_GRID_MIN_VOXELS", str(1 << 18))  # a lone island takes the whole GPU
     from pfsf_b200 import adjoint as AD
     from pfsf_b200 import capi, synth
     import torch
 
-    isl = synth.noise_island((128, 128, 64), seed=41)
-    rng = np.random.default_rng(41)
+    O = _oracle()
     eng = capi.Engine(capi.default_config(max_island_size=1 << 28, tick_budget_ms=1 << 30, vram=180 << 30))
     if eng.init() != capi.PFSF_OK:
         raise RuntimeError("pfsf_init failed")
     eng.set_solve_mode(capi.SOLVE_BATCHED)
     eng.set_precision({"bf16": capi.PREC_BF16, "fp16": capi.PREC_FP16, "fp32": capi.PREC_FP32}[args.precision])
-    sess = AD.Session(eng, 1, isl.dims, isl.vtype, tol=1e-10, max_iter=4000)
     ticks = 32
-    k_target = (isl.kappa * np.exp(0.2 * rng.standard_normal(isl.n))).astype(np.float32)
-    phi_target = sess.solve(k_target, (2.0 * isl.source).astype(np.float32))
-    rcomp = torch.tensor(np.maximum(isl.rcomp.astype(np.float64), 1.0) * 1e6)
-    pt = torch.tensor(phi_target)
+
+    def setup(dims, seed, iid):
+        isl = synth.noise_island(dims, seed=seed)
+        rng = np.random.default_rng(seed)
+        sess = AD.Session(eng, iid, isl.dims, isl.vtype, tol=1e-10, max_iter=4000)
+        k_target = (isl.kappa * np.exp(0.2 * rng.standard_normal(isl.n))).astype(np.float32)
+        phi_target = sess.solve(k_target, isl.source.astype(np.float32))
+        rcomp = np.maximum(isl.rcomp.astype(np.float64), 1.0) * 1e6
+        x2 = sess.solve(isl.kappa, (2.0 * isl.source).astype(np.float32))
+        psi, _ = O.amor_psi64(isl.dims, isl.kappa.astype(np.float64), isl.vtype, x2)
+        return isl, rng, sess, phi_target, rcomp, 0.5 * float(psi.max())
+
+    isl, rng, sess, phi_target, rcomp, hs = setup((128, 128, 64), 41, 1)
     kt = torch.tensor(isl.kappa.astype(np.float64), requires_grad=True)
-    st = torch.tensor(isl.source.astype(np.float64), requires_grad=True)
+    st = torch.tensor(isl.source.astype(np.float64))
     for _ in range(max(args.warmup, 1)):
         sess.solve(isl.kappa, isl.source)
+    sess.recomputes = 0
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    phis, H, ck = AD.ramped_trajectory(sess, kt, st, ticks=ticks, ramp=2.0, checkpoint_every=8)
+    L, phis, H = AD.trajectory_loss(sess, kt, st, rcomp, phi_target, ticks=ticks, ramp=2.0, checkpoint_every=8,
+                                    h_scale=hs)
+    torch.cuda.synchronize()
     t_fwd = (time.perf_counter() - t0) * 1000.0
-    L = AD.calibration_loss(phis[-1], kt, isl.vtype, isl.dims, rcomp, pt)
     t0 = time.perf_counter()
     L.backward()
+    torch.cuda.synchronize()
     t_bwd = (time.perf_counter() - t0) * 1000.0
     adj_stats = sess.last_stats
-    g = kt.grad.numpy()
-    phi_T = phis[-1].detach().numpy()
-
-    dev = torch.device("cuda")
-    rc_d, pt_d = rcomp.to(dev), pt.to(dev)
-
-    def loss_np(phv, kv):
-        with torch.no_grad():
-            return float(AD.calibration_loss(torch.tensor(phv, device=dev), torch.tensor(kv, device=dev), isl.vtype,
-                                             isl.dims, rc_d, pt_d))
-
+    g = kt.grad.detach().cpu().numpy()
     vox = rng.choice(np.where(isl.vtype != 0)[0], args.fd_voxels, replace=False)
-    src_T = (isl.source.astype(np.float32) * np.float32(2.0))
+    phis0 = [p.detach().numpy() for p in phis]
     t0 = time.perf_counter()
-    fd, kink = AD.finite_difference_kappa(sess, isl.kappa, src_T, phi_T, loss_np, vox)
+    fd, kink = AD.trajectory_finite_difference(sess, isl.kappa.astype(np.float32), isl.source, phis0, rcomp,
+                                               phi_target, vox, ramp=2.0, h_scale=hs)
     t_fd = time.perf_counter() - t0
     ok = ~kink
     rel = np.abs(g[vox][ok] - fd[ok]) / np.maximum(np.abs(fd[ok]), 1e-300)
+    # FP64 oracle gradient of the same trajectory loss on a reduced island
+    risl, _, rsess, rpt, rrc, rhs_ = setup((32, 32, 16), 43, 2)
+    rk = torch.tensor(risl.kappa.astype(np.float64), requires_grad=True)
+    Lr, _, _ = AD.trajectory_loss(rsess, rk, torch.tensor(risl.source.astype(np.float64)), rrc, rpt, ticks=8,
+                                  ramp=2.0, checkpoint_every=4, h_scale=rhs_)
+    Lr.backward()
+    Lo, gko, _, _ = O.trajectory_grad64(risl.dims, risl.kappa.astype(np.float64), risl.vtype,
+                                        risl.source.astype(np.float64), rrc, rpt, 8, 2.0, rhs_,
+                                        threads=os.cpu_count() or 1)
+    oracle_err = float(np.abs(rk.grad.detach().cpu().numpy() - gko).max() / np.abs(gko).max())
     line = {
-        "metric": "config-4 adjoint: max rel. error of dL/dkappa vs central FD (non-kink voxels)",
+        "metric": "config-4 adjoint: max rel. error of dL/dkappa of the 32-tick trajectory loss vs central FD "
+                  "(non-kink voxels)",
         "value": float(rel.max()) if rel.size else None, "unit": "relative", "higher_is_better": False,
         "n_gpus": 1, "data": "synthetic", "dtype": "f32",
         "config": {"workload": "one 128x128x64 noise island (60 % occupancy, anchored component), 32 ticks, "
-                               "load ramped 1x->2x, checkpoint every 8 ticks",
+                               "load ramped 1x->2x, checkpoint every 8 ticks, loss over every tick + history term",
                    "active_voxels": int(isl.n_active), "precision": args.precision, "tol": 1e-10},
         "median_rel_error": float(np.median(rel)) if rel.size else None,
         "fd_voxels": int(len(vox)), "kink_hits": int(kink.sum()), "fd_step": 2.0 ** -10,
-        "forward_ms_per_tick": t_fwd / ticks, "backward_ms": t_bwd,
-        "adjoint_device_ms": float(adj_stats.device_ms), "recomputes": sess.recomputes,
-        "loss": float(L.detach()), "fd_seconds": t_fd,
-        "fp64_oracle_gradient": "checked at small sizes by tests/test_gpu_adjoint.py (a CPU FP64 solve of this "
-                                "island takes tens of minutes)",
+        "forward_ms_per_tick": t_fwd / ticks, "backward_ms": t_bwd, "recomputes": sess.recomputes,
+        "adjoint_device_ms_last": float(adj_stats.device_ms), "loss": float(L.detach()), "fd_seconds": t_fd,
+        "fp64_oracle_gradient_error": oracle_err,
+        "fp64_oracle_island": "32x32x16 noise island, 8 ticks, checkpoint every 4 (the same loss)",
     }
     print(json.dumps(line), flush=True)
     eng.close()

@@ -408,6 +408,81 @@ def flux_loss64(dims, kappa, vtype, phi, rcomp, phi_target):
     return L, gphi.reshape(-1), gk.reshape(-1)
 
 
+def amor_psi64(dims, kappa, vtype, phi):
+    """psi_e of the history update (SH/rbgs_smooth.comp.glsl:177-191) in FP64:
+    phi^2 / 2, times 0.01 where the face inflow exceeds three times the face
+    outflow (face conductivity = the harmonic-mean kappa link value); solid
+    voxels with phi > 0 only.  Returns (psi, factor)."""
+    k = _grid(kappa, dims)
+    t = np.asarray(vtype).reshape(k.shape)
+    P = np.where(t == 1, _grid(phi, dims), 0.0)
+    fin = np.zeros_like(P)
+    fout = np.zeros_like(P)
+    lz, ly, lx = k.shape
+    for dx, dy, dz in ((-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)):
+        kj = np.zeros_like(k)
+        tj = np.zeros_like(t)
+        pj = np.zeros_like(P)
+        src, dst = [slice(None)] * 3, [slice(None)] * 3
+        for ax, o in zip((2, 1, 0), (dx, dy, dz)):
+            if o == 1:
+                dst[ax], src[ax] = slice(0, -1), slice(1, None)
+            elif o == -1:
+                dst[ax], src[ax] = slice(1, None), slice(0, -1)
+        kj[tuple(dst)] = k[tuple(src)]
+        tj[tuple(dst)] = t[tuple(src)]
+        pj[tuple(dst)] = P[tuple(src)]
+        ok = (t != 0) & (tj != 0) & ((k + kj) > 0)
+        sig = np.where(ok, 2.0 * k * kj / np.where(ok, k + kj, 1.0), 0.0)
+        flow = sig * (pj - P)
+        fin += np.maximum(flow, 0.0)
+        fout += np.maximum(-flow, 0.0)
+    factor = np.where(fin > 3.0 * fout, 0.01, 1.0)
+    live = (t == 1) & (P > 0)
+    return np.where(live, 0.5 * P * P * factor, 0.0).reshape(-1), np.where(live, factor, 0.0).reshape(-1)
+
+
+def trajectory_grad64(dims, kappa, vtype, source, rcomp, phi_target, ticks, ramp, h_scale, threads=1):
+    """FP64 restatement of the config-4 trajectory loss and its gradient
+    dL/dkappa (the torch tooling's trajectory_loss): per tick t the FP64
+    solution of A(kappa) phi_t = f_t s, the flux / target terms of
+    flux_loss64 with target f_t phi_target, the history H = max_t psi_e(phi_t)
+    with the softplus(H / h_scale - 1) term (its gradient reaching the tick
+    that attains the max), and one FP64 adjoint solve per tick.
+    Returns (L, dL/dkappa, phis, argmax tick per voxel)."""
+    k = np.asarray(kappa, np.float64)
+    s = np.asarray(source, np.float64)
+    solid = np.asarray(vtype) == 1
+    phis, L = [], 0.0
+    gk = np.zeros_like(k)
+    gphis = []
+    H = np.zeros_like(k)
+    arg = np.full(k.size, -1)
+    fac = []
+    for t in range(ticks):
+        f = 1.0 + (ramp - 1.0) * t / max(ticks - 1, 1)
+        x, _, rel = kappa_mgpcg64(dims, k, vtype, f * s, tol=1e-13, threads=threads)
+        phis.append(x)
+        Lt, gphi, gkd = flux_loss64(dims, k, vtype, x, rcomp, f * np.asarray(phi_target, np.float64))
+        L += Lt
+        gk += gkd
+        gphis.append(gphi)
+        psi, fa = amor_psi64(dims, k, vtype, x)
+        fac.append(fa)
+        upd = psi > H
+        arg[upd] = t
+        H = np.maximum(H, psi)
+    z = H / h_scale - 1.0
+    L += float(np.sum(np.where(solid, np.logaddexp(0.0, z), 0.0)))
+    dH = np.where(solid, 1.0 / (1.0 + np.exp(-z)) / h_scale, 0.0)
+    for t in range(ticks):
+        sel = arg == t
+        gphi = gphis[t] + np.where(sel, dH * phis[t] * fac[t], 0.0)
+        _, gke, _ = kappa_adjoint64(dims, k, vtype, phis[t], gphi)
+        gk += gke
+    return L, gk, phis, arg
+
+
 # ------------------------------------------------------------- island labels
 NO_ISLAND = 0xFFFFFFFF
 

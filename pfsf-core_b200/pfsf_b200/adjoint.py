@@ -105,6 +105,159 @@ def calibration_loss(phi, kappa, vtype, dims, rcomp, phi_target):
     return torch.where(solid, torch.nn.functional.softplus(z) + 0.5 * d * d, zero).sum()
 
 
+_FACES = ((-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1))
+
+
+def _shift(a, dx, dy, dz, fill=0.0):
+    """b[z, y, x] = a[z + dz, y + dy, x + dx], fill outside the box."""
+    b = torch.full_like(a, fill)
+    lz, ly, lx = a.shape
+
+    def rng(d, n):
+        return (slice(0, n - 1), slice(1, n)) if d == 1 else ((slice(1, n), slice(0, n - 1)) if d == -1 else
+                                                             (slice(0, n), slice(0, n)))
+    (zo, zi), (yo, yi), (xo, xi) = rng(dz, lz), rng(dy, ly), rng(dx, lx)
+    b[zo, yo, xo] = a[zi, yi, xi]
+    return b
+
+
+def amor_psi(phi, kappa, vtype, dims):
+    """Elastic energy density with the Amor split, as the history update
+    H = max(H, psi_e) computes it (SH/rbgs_smooth.comp.glsl:177-191, the
+    library's k_history): psi_e = phi^2 / 2, times 0.01 where the face inflow
+    exceeds three times the face outflow; flows over the six faces with the
+    face conductivity = the harmonic-mean kappa link value; solid voxels with
+    phi > 0 only (0 elsewhere).  Differentiable in phi (piecewise)."""
+    lx, ly, lz = dims
+    t = torch.as_tensor(np.asarray(vtype), device=phi.device).reshape(lz, ly, lx)
+    k = kappa.reshape(lz, ly, lx).to(phi.dtype)
+    p = torch.where(t == 1, phi.reshape(lz, ly, lx), torch.zeros((), dtype=phi.dtype, device=phi.device))
+    fin = torch.zeros_like(p)
+    fout = torch.zeros_like(p)
+    for dx, dy, dz in _FACES:
+        kj = _shift(k, dx, dy, dz)
+        tj = _shift(t, dx, dy, dz, 0)
+        pj = _shift(p, dx, dy, dz)
+        ok = (t != 0) & (tj != 0) & ((k + kj) > 0)
+        sig = torch.where(ok, 2.0 * k * kj / torch.where(ok, k + kj, torch.ones_like(k)), torch.zeros_like(k))
+        flow = sig * (pj - p)
+        fin = fin + torch.relu(flow)
+        fout = fout + torch.relu(-flow)
+    factor = torch.where(fin > 3.0 * fout, torch.full_like(p, 0.01), torch.ones_like(p))
+    psi = 0.5 * p * p * factor
+    return torch.where((t == 1) & (p > 0), psi, torch.zeros_like(psi)).reshape(-1)
+
+
+def _device(device):
+    if device is not None:
+        return torch.device(device)
+    return torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu")
+
+
+def trajectory_objective(phis, kappa, vtype, dims, rcomp, phi_target, ramp=2.0, h_scale=1.0, device=None):
+    """The config-4 calibration loss of a given trajectory phi_0..phi_{T-1}
+    (tick t under the load f_t, ramped linearly from 1 to `ramp`):
+
+        L = sum_t [ sum_solid softplus(flux_in(phi_t) / rcomp - 1)
+                    + 1/2 sum_solid (phi_t - f_t phi_target)^2 ]
+          + sum_solid softplus(H / h_scale - 1),   H = max_t psi_e(phi_t)
+
+    (psi_e: amor_psi, the history the phase field reads), as torch ops on
+    `device` (the GPU by default).  Returns (L, H)."""
+    dev = _device(device)
+    ticks = len(phis)
+    kd = torch.as_tensor(kappa, device=dev, dtype=torch.float64) if not torch.is_tensor(kappa) else kappa.to(dev)
+    rc = torch.as_tensor(rcomp, device=dev, dtype=torch.float64)
+    pt = torch.as_tensor(phi_target, device=dev, dtype=torch.float64)
+    solid = torch.as_tensor(np.asarray(vtype) == 1, device=dev)
+    L = torch.zeros((), dtype=torch.float64, device=dev)
+    H = torch.zeros(int(np.prod(dims)), dtype=torch.float64, device=dev)
+    for t, phi in enumerate(phis):
+        f = 1.0 + (ramp - 1.0) * t / max(ticks - 1, 1)
+        pd = (phi if torch.is_tensor(phi) else torch.as_tensor(phi, dtype=torch.float64)).to(dev)
+        L = L + calibration_loss(pd, kd, vtype, dims, rc, f * pt)
+        H = torch.maximum(H, amor_psi(pd, kd, vtype, dims))
+    z = H / h_scale - 1.0
+    L = L + torch.where(solid, torch.nn.functional.softplus(z), torch.zeros_like(z)).sum()
+    return L, H
+
+
+def trajectory_loss(session, kappa, source, rcomp, phi_target, ticks=32, ramp=2.0, checkpoint_every=8,
+                    h_scale=1.0, device=None):
+    """Solves the ramped trajectory (tick t: A(kappa) phi_t = f_t s, a
+    checkpoint of phi every `checkpoint_every` ticks) and returns
+    (trajectory_objective, phis, H).  Every tick enters the gradient:
+    backward runs each tick's adjoint in reverse order, and the device holds
+    only the last tick's solution, so every earlier tick is re-solved from
+    its checkpoint first (Session.recomputes counts them)."""
+    checkpoints = {}
+    phis = []
+    warm = None
+    for t in range(ticks):
+        f = 1.0 + (ramp - 1.0) * t / max(ticks - 1, 1)
+        base = checkpoints.get(checkpoint_every * (t // checkpoint_every))
+        phi = KappaSolve.apply(kappa, source * f, session, t, warm if base is None else base)
+        x = phi.detach().numpy()
+        if t % checkpoint_every == 0:
+            checkpoints[t] = x.astype(np.float32)
+        warm = x.astype(np.float32)
+        phis.append(phi)
+    L, H = trajectory_objective(phis, kappa, session.vtype, session.dims, rcomp, phi_target, ramp, h_scale, device)
+    return L, phis, H
+
+
+def trajectory_finite_difference(session, kappa32, source32, phis0, rcomp, phi_target, voxels, ramp=2.0,
+                                 h_scale=1.0, h=2.0 ** -10, device=None):
+    """Central differences of trajectory_objective w.r.t. kappa_i at each
+    voxel i: every tick's perturbed solution is phi0_t + delta_t with
+    A(kappa') delta_t = -(A(kappa') - A(kappa)) phi0_t (see
+    finite_difference_kappa), the whole trajectory's loss evaluated at
+    kappa +/- h e_i.  Returns (fd, kink flags): a kink flag marks a voxel
+    whose +/- trajectories differ in a link's inflow side, a voxel's psi_e
+    switch or the tick that attains the history maximum."""
+    ticks = len(phis0)
+    k64 = kappa32.astype(np.float64)
+    vt = session.vtype
+    out, kinks = [], []
+    for i in voxels:
+        vals, trajs, steps = [], [], []
+        for sgn in (1.0, -1.0):
+            kp = kappa32.copy()
+            kp[i] = np.float32(kappa32[i] + np.float32(sgn * h))
+            steps.append(float(kp[i]) - float(kappa32[i]))
+            traj = []
+            for t in range(ticks):
+                rows = _local_rhs(session.dims, k64, vt, phis0[t], i, float(kp[i]))
+                rhs = np.zeros(session.n, np.float32)
+                for r, v in rows.items():
+                    rhs[r] = v
+                traj.append(phis0[t] + session.solve(kp, rhs, tag=("fd", i, sgn, t)))
+            with torch.no_grad():
+                L, H = trajectory_objective(traj, kp.astype(np.float64), vt, session.dims, rcomp, phi_target, ramp,
+                                            h_scale, device)
+            vals.append(float(L))
+            trajs.append((traj, kp))
+        out.append((vals[0] - vals[1]) / (steps[0] - steps[1]))
+        kink = any(_kink(session.dims, vt, a, b) for a, b in zip(trajs[0][0], trajs[1][0]))
+        if not kink:
+            kink = _history_kink(session, trajs[0], trajs[1], device)
+        kinks.append(kink)
+    return np.array(out), np.array(kinks)
+
+
+def _history_kink(session, ta, tb, device):
+    """The +/- trajectories differ in a psi_e switch or the argmax tick."""
+    pats = []
+    for traj, kp in (ta, tb):
+        kd = torch.as_tensor(kp.astype(np.float64), device=_device(device))
+        psis = torch.stack([amor_psi(torch.as_tensor(p, dtype=torch.float64, device=kd.device), kd, session.vtype,
+                                     session.dims) for p in traj])
+        sq = torch.stack([0.5 * torch.as_tensor(p, dtype=torch.float64, device=kd.device) ** 2 for p in traj])
+        switched = (psis < 0.5 * sq).cpu().numpy()
+        pats.append((switched, torch.argmax(psis, dim=0).cpu().numpy()))
+    return bool(np.any(pats[0][0] != pats[1][0]) or np.any(pats[0][1] != pats[1][1]))
+
+
 # ------------------------------------------------------------------- session
 class Session:
     """One island on an engine, registered for differentiable solves."""

@@ -100,3 +100,23 @@ def test_flux_in_is_the_failure_scan_inflow():
                             w = [1.0, 0.5, 1 / 6][m - 1] * 2 * k[i] * k[j] / (k[i] + k[j])
                             want[i] += w * max(p[j] - p[i], 0.0)
     np.testing.assert_allclose(f, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
+def test_amor_psi_is_the_history_update():
+    """The torch and FP64 psi_e used by the trajectory loss are the history
+    update of the tick (oracle o_history, the restatement of
+    SH/rbgs_smooth.comp.glsl:177-191 on the face conductivity)."""
+    import torch
+    from pfsf_b200 import adjoint as AD
+    isl = synth.noise_island((14, 12, 10), seed=23)
+    rng = np.random.default_rng(23)
+    phi = (rng.uniform(0.0, 2.0, isl.n) * (isl.vtype == 1)).astype(np.float32)
+    sig = synth.face_sigma_from_kappa(isl.dims, isl.vtype, isl.kappa)
+    H = np.zeros(isl.n, np.float32)
+    O.history(isl.dims, phi, sig, isl.vtype, H)
+    k64 = isl.kappa.astype(np.float64)
+    psi64, _ = O.amor_psi64(isl.dims, k64, isl.vtype, phi.astype(np.float64))
+    pt = AD.amor_psi(torch.tensor(phi.astype(np.float64)), torch.tensor(k64), isl.vtype, isl.dims).numpy()
+    sc = float(np.abs(H).max())
+    assert np.abs(psi64 - H).max() <= 1e-5 * sc
+    assert np.abs(pt - psi64).max() <= 1e-12 * sc

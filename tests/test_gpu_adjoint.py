@@ -213,3 +213,41 @@ def test_whole_gpu_tier_matches_oracle(lib_built):
             assert np.abs(gbufs[1] - gs_o).max() <= 1e-6 * np.abs(gs_o).max()
     finally:
         e.close()
+
+
+def test_trajectory_loss_gradient_matches_fp64_oracle_and_fd(eng):
+    """The config-4 trajectory loss (per-tick flux and target terms plus the
+    history term over H = max_t psi_e, psi_e with the Amor split) on a
+    reduced island over 6 ramped ticks, checkpoint every 2: the torch
+    gradient through every tick's device adjoint (5 ticks recomputed from
+    their checkpoints) matches the FP64 oracle's trajectory gradient to 1e-6
+    of its largest entry, and central differences to 1e-4 relative on
+    voxels away from kinks."""
+    eng.set_solve_mode(capi.SOLVE_BATCHED)
+    eng.set_precision(capi.PREC_BF16)
+    isl, k, s, phi, rc, pt = _problem((24, 20, 12), seed=31)
+    k64 = isl.kappa.astype(np.float64)
+    psi, _ = O.amor_psi64(isl.dims, k64, isl.vtype, 2.0 * phi)
+    hs = 0.5 * float(psi.max())  # the history term acts on the most loaded voxels
+    sess = AD.Session(eng, _next_id(), isl.dims, isl.vtype, tol=TOL)
+    kt = torch.tensor(k64, requires_grad=True)
+    st = torch.tensor(isl.source.astype(np.float64))
+    L, phis, H = AD.trajectory_loss(sess, kt, st, rc, pt, ticks=6, ramp=2.0, checkpoint_every=2, h_scale=hs)
+    L.backward()
+    assert sess.recomputes == 5
+    Lo, gko, phis_o, arg = O.trajectory_grad64(isl.dims, k64, isl.vtype, isl.source.astype(np.float64), rc, pt,
+                                               6, 2.0, hs)
+    assert abs(float(L) - Lo) <= 1e-6 * abs(Lo)
+    g = kt.grad.detach().cpu().numpy()
+    assert np.abs(g - gko).max() <= 1e-6 * np.abs(gko).max()
+    assert len(set(arg[arg >= 0].tolist())) >= 1
+    # central differences of the whole trajectory's loss
+    rng = np.random.default_rng(31)
+    vox = rng.choice(np.flatnonzero(isl.vtype != 0), 12, replace=False)
+    phis0 = [p.detach().numpy() for p in phis]
+    fd, kink = AD.trajectory_finite_difference(sess, isl.kappa.astype(np.float32), isl.source, phis0, rc, pt, vox,
+                                               ramp=2.0, h_scale=hs)
+    ok = ~kink
+    assert ok.sum() >= 6
+    rel = np.abs(g[vox][ok] - fd[ok]) / np.maximum(np.abs(fd[ok]), 1e-30)
+    assert rel.max() <= 1e-4, rel
