@@ -80,6 +80,14 @@ PFSF_API pfsf_result pfsf_register_island_kappa(pfsf_engine engine, int32_t isla
 PFSF_API void pfsf_set_precision_mode(pfsf_engine engine, pfsf_precision mode);
 PFSF_API void pfsf_set_solve_mode(pfsf_engine engine, pfsf_solve_mode mode);
 
+/* No counterpart in the reference ABI (its native V-cycle takes two W legs
+ * on the coarse levels, dispatcher_vcycle.cpp:315-340, 373-374).  Multigrid
+ * cycle of the batched tolerance solve's preconditioner: PFSF_MG_V (default)
+ * or PFSF_MG_W, which visits every level below the first coarse level twice.
+ * The per-island plain solve always runs V-cycles. */
+typedef enum { PFSF_MG_V = 0, PFSF_MG_W = 1 } pfsf_mg_cycle;
+PFSF_API void pfsf_set_mg_cycle(pfsf_engine engine, pfsf_mg_cycle cycle);
+
 /* Solves every listed island to rel_tol (max_iter outer iterations at most)
  * and writes phi back to its registered phi array.  Returns PFSF_OK even if
  * some island did not converge (see out->islands_converged). */

@@ -161,6 +161,7 @@ public:
     void set_wind(const pfsf_vec3* w) { wind_ = w ? *w : pfsf_vec3{0, 0, 0}; }
     void set_precision(pfsf_precision p) { precision_ = p; }
     void set_solve_mode(pfsf_solve_mode m) { solve_mode_ = m; }
+    void set_mg_cycle(int c) { mg_cycle_ = c == 1 ? 1 : 0; }
     pfsf_result get_tuning(pfsf_tuning* out) const;
     pfsf_result set_tuning(const pfsf_tuning* in);
 
@@ -251,6 +252,7 @@ private:
     int smoother_ = -1;                   // PFSF_SMOOTHER (-1: mode default)
     int cheb_k_ = 3;                      // PFSF_CHEB_K
     int tuning_source_ = PFSF_TUNING_DEFAULT;
+    int mg_cycle_ = 0;                    // 0 V-cycle, 1 W-cycle (batched tolerance solve)
     void load_tuning();                   // tuning file, then environment overrides (init)
 };
 

@@ -431,6 +431,33 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
         tm.sync();
         team_chebc<P>(A, D, l, tm, false, odd);
     }
+    // W-cycle: a second visit of the levels below level 1 (the reference's
+    // second W leg, dispatcher_vcycle.cpp:315-340, 373-374): smooth level 1
+    // from its current x, restrict its residual, the same descent, tail and
+    // ascent, then prolongate into level 1 and smooth it again
+    if (A.wcycle && l0 >= 2) {
+        team_chebc<P>(A, D, 1, tm, false, false);
+        op_restrictc<P>(A, D, 1, t, T);
+        tm.sync();
+        for (int l = 2; l < l0; l++) {
+            team_chebc<P>(A, D, l, tm, true);
+            op_restrictc<P>(A, D, l, t, T);
+            tm.sync();
+        }
+        if (D.lev[l0].n <= kWarpTailCells) {
+            if (tm.leader_warp()) warp_tail_cheb<P>(A, D, l0);
+            tm.sync();
+        } else {
+            team_chebc<P>(A, D, L - 1, tm, true);
+            for (int s = 1; s < A.coarse_sweeps; s++) team_chebc<P>(A, D, L - 1, tm, false);
+        }
+        for (int l = l0 - 1; l >= 1; l--) {
+            float* xa = A.cx + D.lev[l].off;
+            op_prolongc_to(A, D, l, t, T, A.omega_c, xa, odd ? A.cx2 + D.lev[l].off : xa);
+            tm.sync();
+            team_chebc<P>(A, D, l, tm, false, odd);
+        }
+    }
     c0 = globaltimer();
     vt.coarse += c0 - c1;
     op_prolong0_to(A, D, t, T, A.omega_c, A.z + D.off, odd ? A.q + D.off : A.z + D.off);

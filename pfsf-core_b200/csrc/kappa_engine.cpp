@@ -23,7 +23,7 @@ inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 // Compulsory bytes of the passes one island's solve made: every array a pass
 // reads or writes counted once per pass (what a perfectly cached streaming
 // implementation must move), per grid voxel / coarse cell.
-double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps, int smoother, int cheb_k) {
+double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps, int smoother, int cheb_k, int wcycle) {
     const double kb = prec > 0 ? 2.0 : 4.0;   // preconditioner kappa
     const double cb = prec > 0 ? 2.0 : 4.0;   // coarse coefficient
     const double wf = kb;                     // fine-level weights come from kappa
@@ -44,13 +44,16 @@ double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps, int smoo
         }
         vc += n0 * (wf + 1.0 + 4.0 + 4.0) + (double)d.lev[1].n * 8.0;  // residual + restriction
         vc += n0 * (1.0 + 8.0) + (double)d.lev[1].n * 4.0;    // prolongation
+        double coarse = 0.0;
         for (int l = 1; l < d.nlev - 1; l++) {
             const double nl = (double)d.lev[l].n;
-            vc += (smoother == 1 ? (2.0 * cheb_k) * (cell + 4.0 + 8.0 + 8.0) : 2.0 * nu * (cell + 4.0 + 8.0)) * nl;
-            vc += nl * (cell + 8.0) + (double)d.lev[l + 1].n * 8.0;
-            vc += nl * (4.0 + 8.0) + (double)d.lev[l + 1].n * 4.0;
+            coarse += (smoother == 1 ? (2.0 * cheb_k) * (cell + 4.0 + 8.0 + 8.0) : 2.0 * nu * (cell + 4.0 + 8.0)) * nl;
+            coarse += nl * (cell + 8.0) + (double)d.lev[l + 1].n * 8.0;
+            coarse += nl * (4.0 + 8.0) + (double)d.lev[l + 1].n * 4.0;
         }
-        vc += 2.0 * coarse_sweeps * (double)d.lev[d.nlev - 1].n * (cell + 4.0 + 8.0);
+        coarse += 2.0 * coarse_sweeps * (double)d.lev[d.nlev - 1].n * (cell + 4.0 + 8.0);
+        // a W-cycle visits everything below the fine level twice
+        vc += (wcycle && d.nlev > 2 ? 2.0 : 1.0) * coarse;
     } else {
         vc += 2.0 * coarse_sweeps * n0 * (wf + 1.0 + 8.0 + 4.0);
     }
@@ -238,6 +241,7 @@ KArena Engine::solve_params(double tol, int32_t max_iter) const {
     // batched: Chebyshev smoothing (one stencil pass per step, few barriers);
     // plain: symmetric 8-colour Gauss-Seidel (the RBGS of the reference)
     k.smoother = smoother_ >= 0 ? smoother_ : (batched ? 1 : 0);
+    k.wcycle = (batched && mg_cycle_ == 1) ? 1 : 0;
     k.cheb_k = std::max(1, std::min(4, cheb_k_));
     {
         const double lmax = 2.0, lmin = lmax * 0.1;
@@ -297,7 +301,7 @@ pfsf_result Engine::run_solve(const KArena& k, int64_t& nl) {
     // set, occupancy known) and replayed while the parameters stay the same.
     const std::vector<double> key = {k.tol, k.eta_min, (double)k.max_inner, (double)k.max_outer, (double)k.omega_c,
                                      (double)k.nu, (double)k.coarse_sweeps, (double)k.fp64_dots, (double)k.smoother,
-                                     (double)k.cheb_k, (double)k.prec, (double)nbig, (double)nsmall,
+                                     (double)k.cheb_k, (double)k.wcycle, (double)k.prec, (double)nbig, (double)nsmall,
                                      (double)cluster_size_, (double)num_sms_, (double)nisl};
     *flag = 0;
     if (ngiant == 0 && A.launched && !A.graph_off) {
@@ -363,7 +367,7 @@ void Engine::fill_stats(const KArena& k, const std::vector<KDesc>& res, pfsf_sol
         st.max_iterations = std::max(st.max_iterations, d.inner_iters);
         st.max_rel_residual = std::max(st.max_rel_residual, d.relres);
         st.inner_iterations_total += d.inner_iters;
-        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps, k.smoother, k.cheb_k);
+        st.algorithmic_bytes += solve_bytes(d, k.prec, k.nu, k.coarse_sweeps, k.smoother, k.cheb_k, k.wcycle);
         st.active_voxels += A.active[q];
     }
     if (solve_mode_ == PFSF_SOLVE_BATCHED) {

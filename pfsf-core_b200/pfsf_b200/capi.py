@@ -106,6 +106,9 @@ class TickReport(C.Structure):
                 ("grid_voxels", C.c_double), ("device_ms", C.c_float), ("reserved", C.c_int32)]
 
 
+MG_V, MG_W = 0, 1
+
+
 class Tuning(C.Structure):
     SOURCES = {0: "default", 1: "file", 2: "env", 3: "caller"}
     _fields_ = [("struct_bytes", C.c_int32), ("cluster", C.c_int32), ("cluster_min_voxels", C.c_int64),
@@ -175,6 +178,7 @@ def load():
         "pfsf_last_tick_report": ([E, C.POINTER(TickReport)], C.c_int),
         "pfsf_island_phi_max": ([E, C.c_int32, C.POINTER(C.c_float)], C.c_int),
         "pfsf_get_tuning": ([E, C.POINTER(Tuning)], C.c_int),
+        "pfsf_set_mg_cycle": ([E, C.c_int], None),
         "pfsf_set_tuning": ([E, C.POINTER(Tuning)], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
@@ -374,6 +378,10 @@ class Engine:
 
     def set_solve_mode(self, m):
         self.L.pfsf_set_solve_mode(self.h, m)
+
+    def set_mg_cycle(self, cycle):
+        """MG_V (0) or MG_W (1) for the batched tolerance solve's preconditioner."""
+        self.L.pfsf_set_mg_cycle(self.h, int(cycle))
 
     def set_pcg_enabled(self, on):
         self.L.pfsf_set_pcg_enabled(self.h, int(bool(on)))
