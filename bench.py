@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--island-report", default="",
                     help="write one JSON line per island of the last timed solve (team, iterations, times)")
     ap.add_argument("--precision", choices=["bf16", "fp16", "fp32"], default="bf16")
+    ap.add_argument("--cycle", choices=["v", "w"], default="w",
+                    help="fracture workload: multigrid cycle of the batched solve (the configuration asks for W)")
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
@@ -638,6 +640,7 @@ def run_fracture(args):
         assert eng.register_kappa(iid, phik, src, isl.kappa, isl.vtype) == capi.PFSF_OK
         eng.set_solve_mode(mode)
         eng.set_precision(prec)
+        eng.set_mg_cycle(capi.MG_W if args.cycle == "w" else capi.MG_V)
         if scale is None:  # loads scaled so max phi = 20 at 1x: the phase field and the scan act
             rc, st = eng.solve([iid], tol=1e-6, flags=capi.SOLVE_COLD_START)
             scale = 20.0 / float(np.abs(phik).max())
@@ -668,7 +671,9 @@ def run_fracture(args):
         "config": {"workload": f"one {args.dims.replace(',', 'x')} noise island (55 % occupancy, anchored "
                                f"component), {args.ticks} ticks, load ramped 1x->2x, warm start",
                    "grid_voxels": n, "active_voxels": int(isl.n_active), "precision": args.precision,
-                   "tol": args.tol, "generation_s": t_gen},
+                   "tol": args.tol, "generation_s": t_gen,
+                   "cycle": ("W" if args.cycle == "w" else "V") + "-cycle preconditioner (batched solve; the plain "
+                            "per-island solve runs V-cycles)"},
         "solve_device_ms_mean": float(np.mean(m["dev"])), "inner_iterations_mean": float(np.mean(m["iters"])),
         "max_rel_residual_fp64": m["relres"], "failures_last_tick": m["fails"][-1],
         "failures_first_tick": m["fails"][0], "damage_max": float(m["D"].max()),
