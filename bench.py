@@ -662,6 +662,16 @@ def run_fracture(args):
             rel = max(rel, st.max_rel_residual)
         runs[name] = {"D": eng.debug_field(iid, 2), "fail": eng.debug_field(iid, 3), "wall": wall, "dev": dev,
                       "fails": fails, "iters": iters, "relres": rel}
+        if mode == capi.SOLVE_BATCHED:
+            # one fine-level pass of the whole-GPU tier alone, on this island
+            # (a working set far larger than L2): GB/s of its algorithmic bytes
+            peak, peak_kind = peaks()
+            for pname, pid in (("chebyshev_step", 0), ("matvec", 1)):
+                rc, pms, pbytes = eng.time_pass(iid, pid, 20)
+                if rc == capi.PFSF_OK and pms > 0:
+                    runs[name].setdefault("passes", {})[pname] = {
+                        "ms": pms, "bytes": pbytes, "gbs": pbytes / (pms * 1e-3) / 1e9,
+                        "frac_of_hbm": pbytes / (pms * 1e-3) / 1e9 / peak, "peak": peak, "peak_kind": peak_kind}
         eng.L.pfsf_remove_island(eng.h, iid)
     m = runs["mixed"]
     line = {
@@ -677,6 +687,7 @@ def run_fracture(args):
         "solve_device_ms_mean": float(np.mean(m["dev"])), "inner_iterations_mean": float(np.mean(m["iters"])),
         "max_rel_residual_fp64": m["relres"], "failures_last_tick": m["fails"][-1],
         "failures_first_tick": m["fails"][0], "damage_max": float(m["D"].max()),
+        "fine_passes": m.get("passes"),
     }
     if "plain_fp32" in runs:
         p = runs["plain_fp32"]

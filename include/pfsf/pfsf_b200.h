@@ -314,6 +314,15 @@ PFSF_API pfsf_result pfsf_compact_failures_noalloc(const uint8_t* dev_fail_flags
  * out_ieee.  Allocates its own device memory; n <= 2^26. */
 PFSF_API pfsf_result pfsf_debug_rcp64(const double* in, double* out_rcp64, double* out_ieee, int64_t n);
 
+/* Test access (no counterpart in the reference ABI): one fine-level pass of
+ * the whole-GPU tier on an island of the last batched solve (pass 0: a
+ * Chebyshev smoothing step, 1: the FP32 matvec), repeated `reps` times on
+ * the engine stream; *ms = mean time per pass (CUDA events), *bytes = the
+ * pass's algorithmic bytes (the staged input vector and kappa of every box
+ * cell, the per-solid-voxel arrays once). */
+PFSF_API pfsf_result pfsf_debug_time_pass(pfsf_engine engine, int32_t island_id, int32_t pass, int32_t reps,
+                                          float* ms, double* bytes);
+
 /* The cudaStream_t the engine launches on (for event timing by callers). */
 PFSF_API void* pfsf_get_stream(pfsf_engine engine);
 

@@ -169,6 +169,7 @@ public:
     pfsf_result solve_to_tolerance(const int32_t* ids, int32_t count, double tol, int32_t max_iter, uint32_t flags,
                                    pfsf_solve_stats* out);
     pfsf_result read_solution64(int32_t id, double* out, int64_t cap, int64_t* count);
+    pfsf_result debug_time_pass(int32_t id, int32_t pass, int32_t reps, float* ms, double* bytes);
     pfsf_result island_report(int32_t id, pfsf_island_report* out) const;
     pfsf_result tick_tolerance(const int32_t* ids, int32_t count, void* fail_addr, int64_t fail_bytes, double tol,
                                int32_t max_iter, pfsf_solve_stats* out);

@@ -145,6 +145,11 @@ void free_plain_graphs(PlainGraphs& g);
 // the graph could not be built or launched.
 int64_t solve_plain(cudaStream_t s, const KArena& a, int isl, const KDesc& hdesc, PlainGraphs& cache);
 int batched_threads();
+// One fine-level pass of the whole-GPU tier (0: Chebyshev step, 1: FP32
+// matvec) `reps` times over island isl of the last solve (its lists and
+// inverse diagonal still in the arena); a.queue[8..10] must be zero.
+// Returns 0, -1 on a launch failure.
+int launch_pass(cudaStream_t s, const KArena& a, int isl, int pass, int reps, int num_sms);
 int64_t plain_scratch_floats();
 // Adjoint: b = g on solid voxels, x64 = 0 (kappa_adjoint.cu).
 void launch_adjoint_prepare(cudaStream_t s, const KArena& a, int64_t nfine_total);

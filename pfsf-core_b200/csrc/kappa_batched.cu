@@ -765,7 +765,65 @@ cudaError_t launch_p(cudaStream_t s, const SideStream& side, const KArena& a, in
     return e;
 }
 
+// One fine-level pass of the whole-GPU tier, `reps` times in a row with a
+// grid barrier between repetitions, on island a.order-independent index isl
+// of the last solve (its solid lists and inverse diagonal are still in the
+// arena): pass 0 = one Chebyshev step (zin = z, zout = q), pass 1 = the FP32
+// matvec q = A p.  For measuring a pass alone; the arrays it writes (q, d)
+// are scratch between solves.
+template <int P>
+__global__ void __launch_bounds__(kBatchedThreads, kBatchedMinBlocks)
+    k_pass(const __grid_constant__ KArena A, int isl, int pass, int reps) {
+    __shared__ SharedScratch sh;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    FlatSmem& fs = *reinterpret_cast<FlatSmem*>(dyn_smem);
+    GridTeam tm{&sh, reinterpret_cast<unsigned*>(A.queue + 8), reinterpret_cast<unsigned*>(A.queue + 9), A.queue + 10,
+                reinterpret_cast<double*>(A.scratch), &fs};
+    const KDesc& D = A.desc[isl];
+    for (int r = 0; r < reps; r++) {
+        if (pass == 0) {
+            fop_cheb0_dz<P>(A, D, fs, tm.cta(), tm.ncta(), A.z + D.off, A.q + D.off, A.cheb_c1[1], A.cheb_c2[1]);
+        } else {
+            float pq = 0.0f;
+            fop_matvec(A, D, fs, tm.cta(), tm.ncta(), pq);
+        }
+        tm.sync();
+    }
+}
+
+template <int P>
+cudaError_t launch_pass_p(cudaStream_t s, const KArena& a, int isl, int pass, int reps, int num_sms) {
+    auto kern = k_pass<P>;
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FlatSmem)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchedThreads, sizeof(FlatSmem)) !=
+            cudaSuccess ||
+        per_sm <= 0)
+        return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3(std::min(num_sms * per_sm, kGridMaxBlocks));
+    cfg.blockDim = dim3(kBatchedThreads);
+    cfg.dynamicSmemBytes = sizeof(FlatSmem);
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a, isl, pass, reps);
+}
+
 }  // namespace
+
+int launch_pass(cudaStream_t s, const KArena& a, int isl, int pass, int reps, int num_sms) {
+    cudaError_t e;
+    switch (a.prec) {
+        case 1: e = launch_pass_p<1>(s, a, isl, pass, reps, num_sms); break;
+        case 2: e = launch_pass_p<2>(s, a, isl, pass, reps, num_sms); break;
+        default: e = launch_pass_p<0>(s, a, isl, pass, reps, num_sms); break;
+    }
+    return e == cudaSuccess ? 0 : -1;
+}
 
 int batched_threads() { return kBatchedThreads; }
 

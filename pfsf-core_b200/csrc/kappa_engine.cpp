@@ -588,6 +588,40 @@ pfsf_result Engine::island_report(int32_t id, pfsf_island_report* out) const {
     return PFSF_OK;
 }
 
+pfsf_result Engine::debug_time_pass(int32_t id, int32_t pass, int32_t reps, float* ms, double* bytes) {
+    if (!available_) return PFSF_ERROR_NOT_INIT;
+    if (!ms || !bytes || (pass != 0 && pass != 1) || reps <= 0 || !arena_ || !arena_->solved) return PFSF_ERROR_INVALID_ARG;
+    auto it = std::find(arena_->ids.begin(), arena_->ids.end(), id);
+    if (it == arena_->ids.end()) return PFSF_ERROR_INVALID_ARG;
+    const int q = (int)(it - arena_->ids.begin());
+    const KArena k = solve_params(1e-6, 0);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemsetAsync(k.queue, 0, 16 * sizeof(int), stream_);
+    cudaEventRecord(e0, stream_);
+    const int rc = kappa::launch_pass(stream_, k, q, pass, reps, num_sms_);
+    cudaEventRecord(e1, stream_);
+    int err = 0;
+    cudaMemcpyAsync(&err, k.queue + 10, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+    const bool ok = rc == 0 && CU_OK(cudaStreamSynchronize(stream_)) && err == 0;
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    launches_++;
+    if (!ok) return PFSF_ERROR_VULKAN;
+    // algorithmic bytes: the march stages the input vector and kappa of every
+    // cell of the island's box; the solid voxels read and write the rest
+    const double n = (double)arena_->desc[q].n, na = (double)arena_->active[q];
+    const double kb = k.prec > 0 ? 2.0 : 4.0;
+    const double per = pass == 0 ? (4.0 + kb) * n + (4.0 + 4.0 + 8.0 + 4.0 + 4.0) * na  // r, dinv, d rw, zout, list
+                                 : (4.0 + 4.0) * n + (4.0 + 4.0) * na;                     // p, k32; q, list
+    *ms = t / (float)reps;
+    *bytes = per;
+    return PFSF_OK;
+}
+
 pfsf_result Engine::read_solution64(int32_t id, double* out, int64_t cap, int64_t* count) {
     if (!available_) return PFSF_ERROR_NOT_INIT;
     if (!out || !count) return PFSF_ERROR_INVALID_ARG;

@@ -200,6 +200,12 @@ PFSF_API pfsf_result pfsf_island_phi_max(pfsf_engine e, int32_t id, float* out) 
     return g ? g->island_phi_max(id, out) : PFSF_ERROR_INVALID_ARG;
 }
 
+PFSF_API pfsf_result pfsf_debug_time_pass(pfsf_engine e, int32_t id, int32_t pass, int32_t reps, float* ms,
+                                          double* bytes) {
+    Engine* g = E(e);
+    return g ? g->debug_time_pass(id, pass, reps, ms, bytes) : PFSF_ERROR_INVALID_ARG;
+}
+
 PFSF_API pfsf_result pfsf_last_tick_report(pfsf_engine e, pfsf_tick_report* out) {
     Engine* g = E(e);
     return g ? g->last_tick_report(out) : PFSF_ERROR_INVALID_ARG;

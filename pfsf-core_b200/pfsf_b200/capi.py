@@ -179,6 +179,8 @@ def load():
         "pfsf_island_phi_max": ([E, C.c_int32, C.POINTER(C.c_float)], C.c_int),
         "pfsf_get_tuning": ([E, C.POINTER(Tuning)], C.c_int),
         "pfsf_set_mg_cycle": ([E, C.c_int], None),
+        "pfsf_debug_time_pass": ([E, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_double)],
+                                 C.c_int),
         "pfsf_set_tuning": ([E, C.POINTER(Tuning)], C.c_int),
         "pfsf_get_stream": ([E], C.c_void_p),
         "pfsf_kernel_launch_count": ([E], C.c_int64),
@@ -378,6 +380,12 @@ class Engine:
 
     def set_solve_mode(self, m):
         self.L.pfsf_set_solve_mode(self.h, m)
+
+    def time_pass(self, iid, pass_, reps=10):
+        """pfsf_debug_time_pass: (rc, ms per pass, algorithmic bytes per pass)."""
+        ms, b = C.c_float(0.0), C.c_double(0.0)
+        rc = self.L.pfsf_debug_time_pass(self.h, iid, pass_, reps, C.byref(ms), C.byref(b))
+        return rc, ms.value, b.value
 
     def set_mg_cycle(self, cycle):
         """MG_V (0) or MG_W (1) for the batched tolerance solve's preconditioner."""
