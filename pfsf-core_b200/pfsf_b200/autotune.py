@@ -69,7 +69,7 @@ def _time(eng, ids, tol, reps):
     return float(np.median(ms))
 
 
-def tune(eng, islands=1024, target_active=1.5e7, big_dims=(160, 160, 96), tol=1e-6, reps=3, budget_s=300.0,
+def tune(eng, islands=4096, target_active=6.0e7, big_dims=(160, 160, 96), tol=1e-6, reps=3, budget_s=300.0,
          seed=17, candidates=None, log=None):
     """Coordinate descent over the launch-shape parameters on engine `eng`
     (initialised, batched mode, BF16 storage).  Returns (best tuning dict,
@@ -163,8 +163,8 @@ def write_section(path, key, params, note=""):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_FILE)
-    ap.add_argument("--islands", type=int, default=1024)
-    ap.add_argument("--target-active", type=float, default=1.5e7)
+    ap.add_argument("--islands", type=int, default=4096)
+    ap.add_argument("--target-active", type=float, default=6.0e7)
     ap.add_argument("--budget", type=float, default=300.0)
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args()
