@@ -88,6 +88,16 @@ PFSF_API void pfsf_set_solve_mode(pfsf_engine engine, pfsf_solve_mode mode);
 typedef enum { PFSF_MG_V = 0, PFSF_MG_W = 1 } pfsf_mg_cycle;
 PFSF_API void pfsf_set_mg_cycle(pfsf_engine engine, pfsf_mg_cycle cycle);
 
+/* Replaces the reference's unexported aggregation correction
+ * (NP/src/solver/dispatcher_amg.cpp:83 recordAMGCorrection with the
+ * aggregates of NP/src/solver/amg_builder.cpp:9 buildAMG), which its native
+ * tick declares but never records.  enable != 0: every PCG start of the
+ * reference tick (pfsf_tick_dbb / pfsf_tick) first applies
+ * phi += P D_c^-1 P^T r to the start's residual r, then starts again from the
+ * corrected phi.  Aggregates are rebuilt on the device whenever an island's
+ * inputs are uploaded.  Off by default (the reference tick as recorded). */
+PFSF_API void pfsf_set_amg(pfsf_engine engine, int32_t enable);
+
 /* Solves every listed island to rel_tol (max_iter outer iterations at most)
  * and writes phi back to its registered phi array.  Returns PFSF_OK even if
  * some island did not converge (see out->islands_converged). */
@@ -272,7 +282,9 @@ PFSF_API pfsf_result pfsf_label_components(pfsf_engine engine, const uint8_t* vo
  * {int32 chebyshev_iter, pcg_allocated, mg_allocated, float prev, last macro
  * residual} (20 bytes), and the device copies of the inputs: 6 source
  * (float32 x N), 7 face conductivity (float32 x 6N, SoA), 8 voxel type
- * (uint8 x N), 9 max_phi, 10 rcomp, 11 rtens (float32 x N).  Copies min(bytes, field size); *out_bytes gets the
+ * (uint8 x N), 9 max_phi, 10 rcomp, 11 rtens (float32 x N), 12 aggregate of each voxel
+ * (int32 x N, -1 left out), 13 prolongation weights (float32 x N), 14 coarse diagonal
+ * (float32 per aggregate); 12-14 are empty until pfsf_set_amg's correction first runs.  Copies min(bytes, field size); *out_bytes gets the
  * field size. */
 PFSF_API pfsf_result pfsf_debug_read_field(pfsf_engine engine, int32_t island_id, int32_t field, void* out,
                                            int64_t bytes, int64_t* out_bytes);

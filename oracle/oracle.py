@@ -22,6 +22,7 @@ F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 U8P = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 U32P = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 
 def build() -> str:
@@ -61,6 +62,10 @@ def lib():
         L.pfo_ptr.restype = C.c_void_p
         L.pfo_get_state.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
         L.pfo_set_flags.argtypes = [C.c_void_p, i, i]
+        L.pfo_set_amg.argtypes = [C.c_void_p, i]
+        L.o_amg_build.argtypes = [i, i, i, F32P, U8P, I32P, F32P, F32P]
+        L.o_amg_build.restype = C.c_int64
+        L.o_amg_correct.argtypes = [i, i, i, I32P, F32P, F32P, F32P, F32P, F32P]
         L.o_tick.argtypes = [C.c_void_p]
         L.o_solve_steps.argtypes = [C.c_void_p, i]
         L.o_solve_steps.restype = i
@@ -188,6 +193,28 @@ def tolerance_tick_tail(dims, phi32, case, H, D, fail):
     return macro
 
 
+def amg_build(dims, sigma, vtype):
+    """NP/src/solver/amg_builder.cpp:9-63 -> (aggregation int32[n],
+    weights float32[n], coarse diagonal float32[nc])."""
+    lx, ly, lz = dims
+    n = lx * ly * lz
+    nc = ((lx + 1) // 2) * ((ly + 1) // 2) * ((lz + 1) // 2)
+    agg = np.zeros(n, np.int32)
+    w = np.zeros(n, np.float32)
+    dc = np.zeros(max(nc, 1), np.float32)
+    lib().o_amg_build(lx, ly, lz, _c(sigma, np.float32), _c(vtype, np.uint8), agg, w, dc)
+    return agg, w, dc[:nc]
+
+
+def amg_correct(dims, agg, w, dc, r, phi):
+    """NP/src/solver/dispatcher_amg.cpp:83-161: phi += P D_c^-1 P^T r (in place on phi)."""
+    lx, ly, lz = dims
+    nc = ((lx + 1) // 2) * ((ly + 1) // 2) * ((lz + 1) // 2)
+    ec = np.zeros(max(nc, 1), np.float32)
+    lib().o_amg_correct(lx, ly, lz, _c(agg, np.int32), _c(w, np.float32), _c(np.resize(dc, max(nc, 1)), np.float32),
+                        _c(r, np.float32), phi, ec)
+
+
 # ---------------------------------------------------------------- island state
 class Island:
     """One island with the native engine's per-island device state
@@ -198,11 +225,12 @@ class Island:
               "max_phi": (6, np.float32, 1), "hydration": (7, np.float32, 1), "H": (8, np.float32, 1),
               "D": (9, np.float32, 1), "fail": (10, np.uint32, 1)}
 
-    def __init__(self, lx, ly, lz, pcg_enabled=True, phase_field=True):
+    def __init__(self, lx, ly, lz, pcg_enabled=True, phase_field=True, amg=False):
         self.dims = (int(lx), int(ly), int(lz))
         self.n = lx * ly * lz
         self._h = lib().pfo_create(lx, ly, lz)
         lib().pfo_set_flags(self._h, int(pcg_enabled), int(phase_field))
+        lib().pfo_set_amg(self._h, int(amg))
         self.nmb = ((lx + 7) // 8) * ((ly + 7) // 8) * ((lz + 7) // 8)
 
     def __del__(self):

@@ -20,6 +20,11 @@
  *   o_pcg_dot           SH/pcg_dot.comp.glsl (pass 1 + pass 2)
  *   o_phase_field       SH/phase_field_evolve.comp.glsl:246-364
  *   o_failure_scan      SH/failure_scan.comp.glsl:36-196
+ *   o_amg_build         NP/src/solver/amg_builder.cpp:9-63 (buildAMG)
+ *   o_amg_correct       NP/src/solver/dispatcher_amg.cpp:83-161 over
+ *                       SH/amg_scatter_restrict.comp.glsl:51-60,
+ *                       SH/amg_coarse_jacobi.comp.glsl:33-40,
+ *                       SH/amg_gather_prolong.comp.glsl:44-71
  *   o_tick              NP/src/pfsf_engine.cpp:424-600 with the schedule of
  *                       NP/src/solver/dispatcher.cpp:106-238,
  *                       dispatcher_vcycle.cpp:315-392, dispatcher_pcg.cpp:254-298
@@ -37,6 +42,10 @@
  *     restated as reading r as it was before the dispatch.
  *   - coarse type buffers are uint8 but the shaders declare uint32: restated
  *     as one type per coarse cell (the data the host uploads).
+ *   - amg_scatter_restrict adds into r_c with atomics in no fixed order:
+ *     restated as the sum over the aggregate's voxels in increasing index.
+ *     amg_gather_prolong stages only the first 256 coarse values in shared
+ *     memory yet reads up to 512 from there: restated as the global read.
  *
  * Parity status: the reference publishes no solver outputs (its fixtures
  * hold inputs only), and its arithmetic runs only as Vulkan GLSL, which
@@ -556,6 +565,73 @@ double o_dot(int64_t n, const float *a, const float *b) {
     return acc;
 }
 
+/* ---- aggregation coarse correction ----
+ * amg_builder.cpp:9-63: 2x2x2 aggregates (the L1 coarsening), a voxel left
+ * out (agg -1, weight 0) when it is an anchor or its six face conductivities
+ * sum below 1e-20; weight = diag6 / (sum of diag6 over the aggregate), and
+ * the coarse diagonal D_c = sum of weight^2 * diag6.  All sums in increasing
+ * voxel index (the builder's loop order).  Returns the coarse cell count. */
+int64_t o_amg_build(int lx, int ly, int lz, const float *sigma, const uint8_t *type, int32_t *agg, float *w,
+                    float *dc) {
+    const int64_t n = (int64_t)lx * ly * lz;
+    const int cx = (lx + 1) / 2, cy = (ly + 1) / 2, cz = (lz + 1) / 2;
+    const int64_t nc = (int64_t)cx * cy * cz;
+    float *d6 = (float *)calloc(n > 0 ? n : 1, 4);
+    float *asum = (float *)calloc(nc > 0 ? nc : 1, 4);
+    for (int64_t i = 0; i < n; i++) {
+        float s = 0.0f;
+        for (int d = 0; d < 6; d++) s += sigma[d * n + i];
+        d6[i] = s;
+        agg[i] = -1;
+        w[i] = 0.0f;
+    }
+    for (int64_t j = 0; j < nc; j++) dc[j] = 0.0f;
+    for (int z = 0; z < lz; z++)
+        for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+                const int64_t i = gidx(x, y, z, lx, ly);
+                if (type && type[i] == 2) continue;
+                if (d6[i] < 1e-20f) continue;
+                const int64_t j = (int64_t)(x / 2) + (int64_t)cx * ((y / 2) + (int64_t)cy * (z / 2));
+                agg[i] = (int32_t)j;
+                asum[j] += d6[i];
+            }
+    for (int64_t i = 0; i < n; i++) {
+        const int32_t j = agg[i];
+        if (j < 0) continue;
+        const float s = asum[j];
+        if (s < 1e-20f) continue;
+        const float pi = d6[i] / s;
+        w[i] = pi;
+        const float t = pi * pi;
+        dc[j] += t * d6[i];
+    }
+    free(d6);
+    free(asum);
+    return nc;
+}
+
+/* dispatcher_amg.cpp:83-161: r_c = P^T r (amg_scatter_restrict), e_c = r_c /
+ * D_c where D_c > 1e-20 else 0 (amg_coarse_jacobi), phi += P e_c
+ * (amg_gather_prolong).  ec: nc floats of scratch. */
+void o_amg_correct(int lx, int ly, int lz, const int32_t *agg, const float *w, const float *dc, const float *r,
+                   float *phi, float *ec) {
+    const int64_t n = (int64_t)lx * ly * lz;
+    const int64_t nc = (int64_t)((lx + 1) / 2) * ((ly + 1) / 2) * ((lz + 1) / 2);
+    for (int64_t j = 0; j < nc; j++) ec[j] = 0.0f;
+    for (int64_t i = 0; i < n; i++)
+        if (agg[i] >= 0) {
+            const float c = w[i] * r[i];
+            ec[agg[i]] += c;
+        }
+    for (int64_t j = 0; j < nc; j++) ec[j] = dc[j] > 1e-20f ? ec[j] / dc[j] : 0.0f;
+    for (int64_t i = 0; i < n; i++)
+        if (agg[i] >= 0) {
+            const float c = w[i] * ec[agg[i]];
+            phi[i] += c;
+        }
+}
+
 /* ---- phase_field_evolve.comp.glsl:246-364.  The shader updates dField in
  * place while neighbouring invocations read it (a race); restated as reading
  * every d_j from the field as it was before the pass. ---- */
@@ -681,6 +757,10 @@ typedef struct {
     int32_t pcg_alloc;
     float *r, *rprev, *p, *ap, *invdiag;
     float red[4];
+    /* aggregation correction before the PCG start (off by default) */
+    int32_t amg;
+    int32_t *agg;
+    float *aw, *adc, *aec;
     /* schedule state */
     int32_t chebyshev_iter, pcg_enabled, phase_field;
     float prev_macro, last_macro;
@@ -705,7 +785,8 @@ void pfo_destroy(pfo_island *s) {
     if (!s) return;
     void *ptrs[] = {s->phi, s->src, s->sigma, s->rcomp, s->rtens, s->maxphi, s->hyd, s->H, s->D, s->type,
                     s->fail, s->macro, s->phi1, s->src1, s->sig1, s->phi2, s->src2, s->sig2, s->snap,
-                    s->type1, s->type2, s->r, s->rprev, s->p, s->ap, s->invdiag};
+                    s->type1, s->type2, s->r, s->rprev, s->p, s->ap, s->invdiag, s->agg, s->aw, s->adc,
+                    s->aec};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
     free(s);
 }
@@ -725,6 +806,14 @@ void pfo_get_state(pfo_island *s, int32_t *iout, float *fout) {
 }
 void pfo_set_flags(pfo_island *s, int pcg_enabled, int phase_field) {
     s->pcg_enabled = pcg_enabled; s->phase_field = phase_field;
+}
+void pfo_set_amg(pfo_island *s, int on) {
+    s->amg = on;
+    if (on && !s->agg) {
+        const int64_t nc = (int64_t)((s->lx + 1) / 2) * ((s->ly + 1) / 2) * ((s->lz + 1) / 2);
+        s->agg = calloc(s->n, 4); s->aw = calloc(s->n, 4);
+        s->adc = calloc(nc > 0 ? nc : 1, 4); s->aec = calloc(nc > 0 ? nc : 1, 4);
+    }
 }
 
 static void mg_alloc(pfo_island *s) {
@@ -809,11 +898,22 @@ static int try_vcycle(pfo_island *s, int k, int mg_available, int *mg_dirty) {
     return 1;
 }
 
+/* PCG start (dispatcher_pcg.cpp:254-271).  With the aggregation correction
+ * on: the start's residual drives one correction of phi
+ * (dispatcher_amg.cpp:83-161, "one application per PCG initialization"),
+ * after which the start is taken again from the corrected phi. */
 static void pcg_initial(pfo_island *s) {
     o_pcg_precompute(s->lx, s->ly, s->lz, s->sigma, s->invdiag);
     o_pcg_matvec(s->lx, s->ly, s->lz, s->phi, s->ap, s->sigma, s->type);
     double rz = o_pcg_update(s->lx, s->ly, s->lz, s->phi, s->r, s->r, s->p, s->ap, s->src, s->type, s->sigma,
                              s->invdiag, s->red, 1);
+    if (s->amg) {
+        o_amg_build(s->lx, s->ly, s->lz, s->sigma, s->type, s->agg, s->aw, s->adc);
+        o_amg_correct(s->lx, s->ly, s->lz, s->agg, s->aw, s->adc, s->r, s->phi, s->aec);
+        o_pcg_matvec(s->lx, s->ly, s->lz, s->phi, s->ap, s->sigma, s->type);
+        rz = o_pcg_update(s->lx, s->ly, s->lz, s->phi, s->r, s->r, s->p, s->ap, s->src, s->type, s->sigma,
+                          s->invdiag, s->red, 1);
+    }
     s->red[0] = (float)rz;
 }
 static void pcg_step(pfo_island *s) {

@@ -4,8 +4,8 @@
 #
 #   make -C oracle -f ref.mk
 #
-# Only the CPU translation units are used (compute/, ext/, trace/, diag/):
-# they need no Vulkan and no generated code.  Compiled without FMA
+# Only the CPU translation units are used (compute/, ext/, trace/, diag/,
+# and solver/amg_builder.cpp): they need no Vulkan and no generated code.  Compiled without FMA
 # contraction and without -march, like this library's host code; the
 # reference's own build adds -march=x86-64-v3, whose FMA contraction the Java
 # side it mirrors does not have.  -Bsymbolic keeps the library's calls to
@@ -20,11 +20,17 @@ CXXFLAGS := -O2 -std=c++17 -fPIC -ffp-contract=off -w -I$(REF)/include -DPFSF_AB
 SRCS := $(wildcard $(REF)/src/compute/*.cpp) $(REF)/src/ext/augmentation.cpp $(REF)/src/ext/hooks.cpp \
         $(REF)/src/ext/plan_dispatcher.cpp $(REF)/src/trace/ring_buffer.cpp $(REF)/src/diag/crash.cpp
 
-all: $(OUT)/libpfsf_ref.so
+all: $(OUT)/libpfsf_ref.so $(OUT)/libpfsf_ref_amg.so
 
 $(OUT)/libpfsf_ref.so: $(SRCS)
 	mkdir -p $(OUT)
 	$(CXX) $(CXXFLAGS) -shared -Wl,-Bsymbolic -o $@ $(SRCS) -lpthread
+
+# the reference's aggregation builder (solver/amg_builder.cpp: standard C++
+# only) behind a C entry point of this directory's own (ref_amg_shim.cpp)
+$(OUT)/libpfsf_ref_amg.so: $(REF)/src/solver/amg_builder.cpp ref_amg_shim.cpp
+	mkdir -p $(OUT)
+	$(CXX) $(CXXFLAGS) -I$(REF)/src/solver -shared -o $@ $^
 
 clean:
 	rm -rf $(OUT)

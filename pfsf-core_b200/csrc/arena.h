@@ -2,6 +2,7 @@
 #pragma once
 #include <vector>
 
+#include "arena_io.h"
 #include "engine.h"
 #include "kappa.h"
 
@@ -18,7 +19,13 @@ struct Engine::Arena {
     KArena dev{};                    // device pointers (into base)
     float* hscratch = nullptr;       // pinned host words (the whole-GPU tier's barrier error flag)
     float* phi_out = nullptr;        // FP32 solution staging (device), aliases e
-    std::vector<void*> pinned;       // host ranges registered for fast copies
+    std::vector<void*> pinned;       // host ranges registered (mapped) by this arena
+    // the islands' kappa-form host arrays as device-mapped addresses, for the
+    // one-launch gather of the inputs and scatter of the solution
+    std::vector<kappa::IslandIO> io;
+    kappa::IslandIO* d_io = nullptr; // device copy (inside base)
+    int io_blocks = 0;               // blocks of the gather / scatter launches
+    bool io_any = false;             // at least one island is mapped
     bool solved = false;             // x64 holds a forward solution of this island set
     int persistent_ctas = 0;         // CTAs of the last batched launch(es)
     bool b_stale = false;            // b holds an adjoint right-hand side, not the sources

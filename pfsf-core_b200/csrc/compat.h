@@ -43,6 +43,10 @@ struct CIsl {
     float *phi1[2], *src1, *sig1, *phi2[2], *src2, *sig2;
     uint8_t *type1, *type2;
     float *r[2], *p, *ap, *invdiag, *partial, *red;
+    // aggregation correction (nullptr / 0: not part of this tick)
+    int32_t* agg;
+    float *aw, *adc, *aec;
+    int64_t anc;           // aggregates: ceil(lx/2) ceil(ly/2) ceil(lz/2)
     // caller's host arrays as device-visible pointers (nullptr: not uploaded
     // by the batched upload; h_curing nullptr keeps hydration)
     const float *h_phi, *h_src, *h_sigma, *h_rcomp, *h_rtens, *h_maxphi, *h_curing;
@@ -53,8 +57,8 @@ struct CIsl {
 };
 
 // Block-count kinds of a batched launch: grid voxels, the voxels of each of
-// the 8 colours, the two coarse levels, macro blocks.
-enum BKind : int { kbN = 0, kbC0 = 1, kbN1 = 9, kbN2 = 10, kbMB = 11, kbKinds = 12 };
+// the 8 colours, the two coarse levels, macro blocks, aggregates.
+enum BKind : int { kbN = 0, kbC0 = 1, kbN1 = 9, kbN2 = 10, kbMB = 11, kbAG = 12, kbKinds = 13 };
 
 // One island group as the launchers see it.
 struct BGroup {
@@ -85,6 +89,13 @@ void pcg_matvec(cudaStream_t s, const BGroup& g, int which);
 void pcg_update(cudaStream_t s, const BGroup& g, int is_init, int fr);
 void finalize(cudaStream_t s, const BGroup& g, int slot, int rotate);
 void pcg_direction(cudaStream_t s, const BGroup& g, int fr);
+// aggregation correction (dispatcher_amg.cpp:83-161): the aggregates,
+// weights and coarse diagonal from sigma and type (amg_builder.cpp:9-63);
+// e_c = (P^T r) / D_c per aggregate from the PCG start's residual slot fr;
+// phi += P e_c
+void amg_build(cudaStream_t s, const BGroup& g);
+void amg_coarse(cudaStream_t s, const BGroup& g, int fr);
+void amg_prolong(cudaStream_t s, const BGroup& g);
 void copy_damage(cudaStream_t s, const BGroup& g);
 void phase_field(cudaStream_t s, const BGroup& g, float l0, float gc, float relax, int split);
 void history(cudaStream_t s, const BGroup& g);

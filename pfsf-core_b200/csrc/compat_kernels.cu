@@ -564,6 +564,99 @@ __device__ __forceinline__ void d_pcg_direction(int lx, int ly, int lz, const fl
     p[i] = np;
 }
 
+// ---- aggregation correction (NP/src/solver/dispatcher_amg.cpp:83-161)
+//
+// An aggregate is the 2x2x2 block of the L1 coarsening (amg_builder.cpp:9-63).
+// One thread per aggregate visits its voxels (2cx+dx, 2cy+dy, 2cz+dz) in
+// increasing voxel index, the order of the builder's sequential loops, so
+// every sum below adds in the reference builder's order.  The restriction
+// gathers instead of the shader's atomic scatter (amg_scatter_restrict
+// adds in no fixed order): no zero fill, no atomics, one deterministic sum.
+__device__ __forceinline__ bool amg_voxel(int lx, int ly, int lz, int cx, int cy, int cz, int k, int64_t& i) {
+    const int x = 2 * cx + (k & 1), y = 2 * cy + ((k >> 1) & 1), z = 2 * cz + (k >> 2);
+    if (x >= lx || y >= ly || z >= lz) return false;
+    i = x + (int64_t)lx * (y + (int64_t)ly * z);
+    return true;
+}
+
+// amg_builder.cpp:23-61: diag6 = sum of the six face conductivities; a
+// voxel joins its aggregate unless it is an anchor or diag6 < 1e-20; weight
+// = diag6 / (aggregate's diag6 sum); D_c = sum of weight^2 * diag6.
+__device__ __forceinline__ void d_amg_build(int lx, int ly, int lz, const float* __restrict__ sigma,
+                                            const uint8_t* __restrict__ type, int32_t* __restrict__ agg,
+                                            float* __restrict__ w, float* __restrict__ dc, int64_t gt_) {
+    const int ax = (lx + 1) >> 1, ay = (ly + 1) >> 1, az = (lz + 1) >> 1;
+    const int64_t j = gt_;
+    if (j >= (int64_t)ax * ay * az) return;
+    const int cx = (int)(j % ax);
+    const int64_t rem = j / ax;
+    const int cy = (int)(rem % ay), cz = (int)(rem / ay);
+    const int64_t n = (int64_t)lx * ly * lz;
+    float d6[8];
+    float asum = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        int64_t i;
+        d6[k] = -1.0f;
+        if (!amg_voxel(lx, ly, lz, cx, cy, cz, k, i)) continue;
+        float t = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 6; d++) t = __fadd_rn(t, sigma[d * n + i]);
+        const bool in = type[i] != 2 && !(t < 1e-20f);
+        agg[i] = in ? (int32_t)j : -1;
+        w[i] = 0.0f;
+        if (in) {
+            asum = __fadd_rn(asum, t);
+            d6[k] = t;
+        }
+    }
+    float dcj = 0.0f;
+    if (!(asum < 1e-20f)) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            int64_t i;
+            if (d6[k] < 0.0f || !amg_voxel(lx, ly, lz, cx, cy, cz, k, i)) continue;
+            const float pi = __fdiv_rn(d6[k], asum);
+            w[i] = pi;
+            dcj = __fadd_rn(dcj, __fmul_rn(__fmul_rn(pi, pi), d6[k]));
+        }
+    }
+    dc[j] = dcj;
+}
+
+// amg_scatter_restrict.comp.glsl:51-60 + amg_coarse_jacobi.comp.glsl:33-40:
+// e_c = (sum of w_i r_i over the aggregate) / D_c, 0 where D_c <= 1e-20
+__device__ __forceinline__ void d_amg_coarse(int lx, int ly, int lz, const int32_t* __restrict__ agg,
+                                             const float* __restrict__ w, const float* __restrict__ dc,
+                                             const float* __restrict__ r, float* __restrict__ ec, int64_t gt_) {
+    const int ax = (lx + 1) >> 1, ay = (ly + 1) >> 1, az = (lz + 1) >> 1;
+    const int64_t j = gt_;
+    if (j >= (int64_t)ax * ay * az) return;
+    const int cx = (int)(j % ax);
+    const int64_t rem = j / ax;
+    const int cy = (int)(rem % ay), cz = (int)(rem / ay);
+    float rc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        int64_t i;
+        if (!amg_voxel(lx, ly, lz, cx, cy, cz, k, i) || agg[i] < 0) continue;
+        rc = __fadd_rn(rc, __fmul_rn(w[i], r[i]));
+    }
+    const float d = dc[j];
+    ec[j] = d > 1e-20f ? __fdiv_rn(rc, d) : 0.0f;
+}
+
+// amg_gather_prolong.comp.glsl:44-71: phi += w e_c[agg] at aggregated voxels
+__device__ __forceinline__ void d_amg_prolong(int64_t n, const int32_t* __restrict__ agg,
+                                              const float* __restrict__ w, const float* __restrict__ ec,
+                                              float* __restrict__ phi, int64_t gt_) {
+    const int64_t i = gt_;
+    if (i >= n) return;
+    const int32_t a = agg[i];
+    if (a < 0) return;
+    phi[i] = __fadd_rn(phi[i], __fmul_rn(w[i], ec[a]));
+}
+
 // Single-block sum of `count` partials into red[slot].  rotate: first copy
 // red[2] -> red[0] (the rTz slot rotation of dispatcher_pcg.cpp recordReductionRotate).
 __device__ __forceinline__ void d_finalize(const float* __restrict__ partial, int64_t count,
@@ -976,6 +1069,21 @@ __global__ void __launch_bounds__(kBlock) kb_pcg_direction(const CIsl* __restric
     BATCH_ISLAND
     d_pcg_direction(I.lx, I.ly, I.lz, I.r[(I.rcur + fr) & 1], I.p, I.type, I.red, I.sigma, t_, lb_);
 }
+__global__ void __launch_bounds__(kBlock) kb_amg_build(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                       int nisl) {
+    BATCH_ISLAND
+    d_amg_build(I.lx, I.ly, I.lz, I.sigma, I.type, I.agg, I.aw, I.adc, t_);
+}
+__global__ void __launch_bounds__(kBlock) kb_amg_coarse(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                        int nisl, int fr) {
+    BATCH_ISLAND
+    d_amg_coarse(I.lx, I.ly, I.lz, I.agg, I.aw, I.adc, I.r[(I.rcur + fr) & 1], I.aec, t_);
+}
+__global__ void __launch_bounds__(kBlock) kb_amg_prolong(const CIsl* __restrict__ tab, const int* __restrict__ bs,
+                                                         int nisl) {
+    BATCH_ISLAND
+    d_amg_prolong(I.n, I.agg, I.aw, I.aec, I.phi, t_);
+}
 __global__ void __launch_bounds__(kBlock) kb_copy_damage(const CIsl* __restrict__ tab, const int* __restrict__ bs,
                                                          int nisl) {
     BATCH_ISLAND
@@ -1092,6 +1200,7 @@ int64_t batch_blocks(const CIsl& I, int kind) {
     if (kind == kbN1) return ceil_div64(I.n1, kBlock);
     if (kind == kbN2) return ceil_div64(I.n2, kBlock);
     if (kind == kbMB) return ceil_div64(I.nmb, kBlock);
+    if (kind == kbAG) return ceil_div64(I.anc, kBlock);
     return 0;
 }
 
@@ -1123,6 +1232,9 @@ void downsample(cudaStream_t s, const BGroup& g, int level) { BLAUNCH(level == 1
 void pcg_precompute(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_pcg_precompute); }
 void pcg_matvec(cudaStream_t s, const BGroup& g, int which) { BLAUNCH(kbN, kb_pcg_matvec, which); }
 void pcg_update(cudaStream_t s, const BGroup& g, int is_init, int fr) { BLAUNCH(kbN, kb_pcg_update, is_init, fr); }
+void amg_build(cudaStream_t s, const BGroup& g) { BLAUNCH(kbAG, kb_amg_build); }
+void amg_coarse(cudaStream_t s, const BGroup& g, int fr) { BLAUNCH(kbAG, kb_amg_coarse, fr); }
+void amg_prolong(cudaStream_t s, const BGroup& g) { BLAUNCH(kbN, kb_amg_prolong); }
 void finalize(cudaStream_t s, const BGroup& g, int slot, int rotate) {
     if (g.nisl > 0) kb_finalize<<<(unsigned)g.nisl, kBlock, 0, s>>>(g.tab, slot, rotate);
 }

@@ -342,6 +342,7 @@ bool Engine::upload(Island& s) {
     if (h.lookups_registered && h.curing)
         ok &= CU_OK(cudaMemcpyAsync(s.hyd, h.curing, n * 4, cudaMemcpyHostToDevice, stream_));
     s.mg_dirty = true;
+    s.amg_dirty = true;
     return ok;
 }
 
@@ -379,6 +380,22 @@ bool Engine::ensure_pcg(Island& s) {
     return true;
 }
 
+// island_buffer.cpp:285-310 allocateAMG: aggregation (int32 per voxel),
+// prolongation weights, coarse diagonal and coarse correction
+bool Engine::ensure_amg(Island& s) {
+    if (s.amg_alloc) return true;
+    s.amg_nc = (int64_t)((s.lx + 1) / 2) * ((s.ly + 1) / 2) * ((s.lz + 1) / 2);
+    bool ok = true;
+    auto F = [&](int64_t c) { void* p = dalloc(s, (size_t)std::max<int64_t>(c, 1) * 4); ok &= p != nullptr; return p; };
+    s.agg = (int32_t*)F(s.n);
+    s.aw = (float*)F(s.n);
+    s.adc = (float*)F(s.amg_nc);
+    s.aec = (float*)F(s.amg_nc);
+    if (!ok) return false;
+    s.amg_alloc = true;
+    s.amg_dirty = true;
+    return true;
+}
 
 
 
@@ -524,6 +541,9 @@ pfsf_result Engine::debug_read_field(int32_t id, int32_t field, void* out, int64
         case 9: src = s->maxphi; size = s->n * 4; break;
         case 10: src = s->rcomp; size = s->n * 4; break;
         case 11: src = s->rtens; size = s->n * 4; break;
+        case 12: src = s->agg; size = s->amg_alloc ? s->n * 4 : 0; break;
+        case 13: src = s->aw; size = s->amg_alloc ? s->n * 4 : 0; break;
+        case 14: src = s->adc; size = s->amg_alloc ? s->amg_nc * 4 : 0; break;
         default: return PFSF_ERROR_INVALID_ARG;
     }
     *out_bytes = size;
@@ -567,6 +587,7 @@ pfsf_result Engine::notify_sparse(int32_t id, int32_t count) {
     s->dirty = true;
     if (!ok) return PFSF_ERROR_VULKAN;
     s->mg_dirty = true;
+    s->amg_dirty = true;
     return PFSF_OK;
 }
 

@@ -109,6 +109,13 @@ struct Island {
           *red = nullptr;
     int rcur = 0;
 
+    // aggregation coarse correction at the PCG start (reference
+    // island_buffer.h:96-103, built from sigma and type on the device)
+    bool amg_alloc = false, amg_dirty = true;
+    int64_t amg_nc = 0;
+    int32_t* agg = nullptr;
+    float *aw = nullptr, *adc = nullptr, *aec = nullptr;
+
     // sparse upload region (pinned host) + device staging
     void* sparse_host = nullptr;
     void* sparse_dev = nullptr;
@@ -162,6 +169,7 @@ public:
     void set_precision(pfsf_precision p) { precision_ = p; }
     void set_solve_mode(pfsf_solve_mode m) { solve_mode_ = m; }
     void set_mg_cycle(int c) { mg_cycle_ = c == 1 ? 1 : 0; }
+    void set_amg(bool on) { amg_enabled_ = on; }
     pfsf_result get_tuning(pfsf_tuning* out) const;
     pfsf_result set_tuning(const pfsf_tuning* in);
 
@@ -219,6 +227,7 @@ private:
     bool upload(Island& isl);
     bool ensure_mg(Island& isl);
     bool ensure_pcg(Island& isl);
+    bool ensure_amg(Island& isl);
     void free_island(Island& isl);
 
     pfsf_config cfg_;
@@ -228,6 +237,7 @@ private:
     kappa::SideStream side_{nullptr, nullptr, nullptr};
     std::map<int32_t, std::unique_ptr<Island>> islands_;
     bool pcg_enabled_ = true;
+    bool amg_enabled_ = false;            // aggregation correction at the PCG start
     pfsf_vec3 wind_{0, 0, 0};
     pfsf_precision precision_ = PFSF_PREC_FP32;
     pfsf_solve_mode solve_mode_ = PFSF_SOLVE_PER_ISLAND;

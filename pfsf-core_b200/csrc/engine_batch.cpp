@@ -41,6 +41,8 @@ struct Plan {
     int extra;     // a second V-cycle when the aspect ratio is >= 8 (dispatcher.cpp:233)
     int mg;        // V-cycles this tick (multigrid available and the cadence reached)
     int mg_dirty;  // coarse conductivity / type rebuilt at the first V-cycle
+    int amg;       // aggregation correction at the PCG start (dispatcher_amg.cpp:83)
+    int amg_build; // aggregates rebuilt from sigma / type first
     bool operator<(const Plan& o) const { return std::memcmp(this, &o, sizeof(Plan)) < 0; }
     bool operator==(const Plan& o) const { return std::memcmp(this, &o, sizeof(Plan)) == 0; }
 };
@@ -69,6 +71,10 @@ double tick_bytes(const Island& s, const Plan& p, bool tail_only, bool phase, bo
         b += sweeps * sweep * n + vcycles * vc;
         if (p.mg_dirty) b += 25.0 * n + 50.0 * n1 + 25.0 * n2;
         if (p.pcg) b += (28.0 + 33.0 + 41.0) * n + p.pc * (33.0 + 53.0 + 37.0) * n;
+        // aggregation correction: build (sigma, type; agg, w), coarse (agg, w, r),
+        // prolong (agg, w, phi rw), then the PCG start again (matvec, update)
+        if (p.amg_build) b += 33.0 * n;
+        if (p.amg) b += 12.0 * n + 16.0 * n + (33.0 + 41.0) * n;
     }
     if (phase) b += 8.0 * n + 47.0 * n;
     b += 42.0 * n;               // failure pass (codes, residual and phi maxima, block counts)
@@ -136,7 +142,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
             s.tuple_cap = need;
         }
         if (tail_only) {
-            if (uploads(s)) s.mg_dirty = true;
+            if (uploads(s)) s.mg_dirty = s.amg_dirty = true;
             plan[k] = p;
             continue;
         }
@@ -165,8 +171,13 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
             if (!ensure_mg(s)) return PFSF_ERROR_OUT_OF_VRAM;
             s.mg_dirty = true;
         }
-        if (s.hosts.registered) s.mg_dirty = true;  // the upload below refreshes the fine inputs
+        if (s.hosts.registered) s.mg_dirty = s.amg_dirty = true;  // the upload below refreshes the fine inputs
         p.mg_dirty = (p.mg && s.mg_dirty) ? 1 : 0;
+        if (p.pcg && amg_enabled_) {
+            if (!ensure_amg(s)) return PFSF_ERROR_OUT_OF_VRAM;
+            p.amg = 1;
+            p.amg_build = s.amg_dirty ? 1 : 0;
+        }
         plan[k] = p;
     }
 
@@ -246,6 +257,10 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
             c.r[0] = s.r[0]; c.r[1] = s.r[1]; c.p = s.p; c.ap = s.ap; c.invdiag = s.invdiag; c.partial = s.partial;
             c.red = s.red;
         }
+        if (plan[k].amg) {
+            c.agg = s.agg; c.aw = s.aw; c.adc = s.adc; c.aec = s.aec;
+            c.anc = s.amg_nc;
+        }
         const HostBuffers& h = s.hosts;
         const bool mapped = uploads(s) && h.m_phi && h.m_source && h.m_cond && h.m_type && h.m_rcomp && h.m_rtens &&
                             h.m_maxphi && (!(h.lookups_registered && h.curing) || h.m_curing);
@@ -299,7 +314,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
     for (int q = 0; q < ng; q++) {
         const Plan& p = plan[order[groups[q].first]];
         key.push_back(groups[q].second - groups[q].first);
-        key.insert(key.end(), {p.pcg, p.rb, p.pc, p.interval, p.extra, p.mg, p.mg_dirty});
+        key.insert(key.end(), {p.pcg, p.rb, p.pc, p.interval, p.extra, p.mg, p.mg_dirty, p.amg, p.amg_build});
     }
     for (int j = 0; j < nisl; j++) {
         const compat::CIsl& c = B.h_tab[j];
@@ -402,8 +417,22 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
                 compat::batch::pcg_precompute(st, g);
                 compat::batch::pcg_matvec(st, g, 0);
                 compat::batch::pcg_update(st, g, 1, ef.fr);
+                nl += 3;
+                if (p.amg) {
+                    // dispatcher_amg.cpp:83-161 from the start's residual, then
+                    // the start again from the corrected phi
+                    if (p.amg_build) {
+                        compat::batch::amg_build(st, g);
+                        nl++;
+                    }
+                    compat::batch::amg_coarse(st, g, ef.fr);
+                    compat::batch::amg_prolong(st, g);
+                    compat::batch::pcg_matvec(st, g, 0);
+                    compat::batch::pcg_update(st, g, 1, ef.fr);
+                    nl += 4;
+                }
                 compat::batch::finalize(st, g, 0, 0);
-                nl += 4;
+                nl++;
                 for (int k = 0; k < p.pc; k++) {
                     compat::batch::pcg_matvec(st, g, 1);
                     compat::batch::finalize(st, g, 1, k == 0 ? 0 : 1);
@@ -485,6 +514,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
             s.cur2 = (s.cur2 + ef.f2) & 1;
             s.rcur = (s.rcur + ef.fr) & 1;
             if (ef.downsampled) s.mg_dirty = false;
+            if (plan[order[j]].amg_build) s.amg_dirty = false;
         }
     }
     return PFSF_OK;

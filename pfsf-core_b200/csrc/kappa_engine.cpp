@@ -12,13 +12,36 @@ namespace pfsf_b200 {
 
 #define CU_OK(expr) (cudaSuccess == (expr))
 
-namespace kappa {
-void launch_to_f32(cudaStream_t s, const KArena& a, int64_t n);
-}
-
 namespace {
 constexpr int64_t kAlignElems = 32;
 inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+inline int64_t ceil_div64(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Device-visible address of a caller's kappa-form host array for the arena's
+// gather / scatter: the island's own earlier mapping when one covers the
+// range (the reference-layout phi can be the same array), else a new mapped
+// registration owned by the arena (unregistered with it); nullptr when the
+// range cannot be mapped (already registered by someone else), and the
+// island is then copied with cudaMemcpyAsync.
+const void* map_arena_host(Island& s, void* p, int64_t bytes, std::vector<void*>& owned) {
+    if (!p || bytes <= 0) return nullptr;
+    const char* a = static_cast<const char*>(p);
+    for (const Island::HostPin& h : s.host_pins) {
+        const char* b = static_cast<const char*>(h.host);
+        if (a >= b && a + bytes <= b + h.bytes) return static_cast<const char*>(h.dev) + (a - b);
+    }
+    if (cudaHostRegister(p, (size_t)bytes, cudaHostRegisterMapped) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    owned.push_back(p);
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess || !d) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return d;
+}
 
 // Compulsory bytes of the passes one island's solve made: every array a pass
 // reads or writes counted once per pass (what a perfectly cached streaming
@@ -151,7 +174,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
                  o_order = take(sizeof(int) * nisl), o_queue = take(256),
                  o_scr = take(sizeof(float) * kappa::plain_scratch_floats()), o_dinv = take(fine * 4),
                  o_d0 = take(fine * 4), o_cdd = take(coarse * 4), o_cx2 = take(coarse * 4),
-                 o_flist = take(fine * 4), o_fstart = take((size_t)std::max<int64_t>(starts, 1) * 4);
+                 o_flist = take(fine * 4), o_fstart = take((size_t)std::max<int64_t>(starts, 1) * 4),
+                 o_io = take(sizeof(kappa::IslandIO) * nisl);
     A->bytes = off;
     if (fault_alloc_after_ >= 0 && alloc_count_ >= fault_alloc_after_) return false;
     if (cudaMalloc(&A->base, A->bytes) != cudaSuccess) {
@@ -201,17 +225,34 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return A->desc[a].n > A->desc[c].n; });
     cudaMemcpyAsync(const_cast<int*>(k.order), order.data(), sizeof(int) * nisl, cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(k.desc, A->desc.data(), sizeof(KDesc) * nisl, cudaMemcpyHostToDevice, stream_);
-    for (Island* s : set) {
+    A->io.assign(nisl, kappa::IslandIO{});
+    int64_t io_blocks = 0;
+    for (int q = 0; q < nisl; q++) {
+        Island* s = set[q];
         const HostBuffers& h = s->hosts;
-        const void* ptrs[4] = {h.k_phi, h.k_source, h.k_kappa, h.k_type};
-        const size_t sz[4] = {(size_t)s->n * 4, (size_t)s->n * 4, (size_t)s->n * 4, (size_t)s->n};
-        for (int q = 0; q < 4; q++) {
-            if (cudaHostRegister(const_cast<void*>(ptrs[q]), sz[q], cudaHostRegisterDefault) == cudaSuccess)
-                A->pinned.push_back(const_cast<void*>(ptrs[q]));
-            else
-                cudaGetLastError();
+        void* ptrs[4] = {h.k_type, h.k_kappa, h.k_source, h.k_phi};
+        const int64_t sz[4] = {s->n, s->n * 4, s->n * 4, s->n * 4};
+        const void* dev[4];
+        bool all = true;
+        for (int t = 0; t < 4; t++) all &= (dev[t] = map_arena_host(*s, ptrs[t], sz[t], A->pinned)) != nullptr;
+        kappa::IslandIO& o = A->io[q];
+        if (all) {
+            o.h_type = static_cast<const uint8_t*>(dev[0]);
+            o.h_kappa = static_cast<const float*>(dev[1]);
+            o.h_source = static_cast<const float*>(dev[2]);
+            o.h_phi = static_cast<const float*>(dev[3]);
+            o.h_phi_out = static_cast<float*>(const_cast<void*>(dev[3]));
+            A->io_any = true;
         }
+        o.off = A->desc[q].off;
+        o.n = s->n;
+        o.b0 = (int32_t)io_blocks;
+        io_blocks += ceil_div64(s->n, kappa::kArenaIoBlock);
     }
+    if (io_blocks > INT32_MAX) return false;
+    A->io_blocks = (int)io_blocks;
+    A->d_io = reinterpret_cast<kappa::IslandIO*>(b + o_io);
+    cudaMemcpyAsync(A->d_io, A->io.data(), sizeof(kappa::IslandIO) * nisl, cudaMemcpyHostToDevice, stream_);
     if (!CU_OK(cudaStreamSynchronize(stream_))) return false;
     arena_ = std::move(A);
     return true;
@@ -417,7 +458,14 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], stream_);
     if (do_upload) {
+        // mapped islands in one gather launch, the others by copies
+        if (A.io_any) {
+            kappa::launch_arena_upload(stream_, A.d_io, (int)set.size(), A.io_blocks, const_cast<uint8_t*>(k.type),
+                                       const_cast<float*>(k.k32), const_cast<float*>(k.b), k.e);
+            launches_++;
+        }
         for (size_t q = 0; q < set.size(); q++) {
+            if (A.io[q].h_type) continue;
             const Island* s = set[q];
             const KDesc& d = A.desc[q];
             const size_t n = (size_t)s->n;
@@ -442,10 +490,12 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     if (pfsf_result rc = run_solve(k, nl); rc != PFSF_OK) return rc;
     cudaEventRecord(ev[2], stream_);
     if (!(flags & PFSF_SOLVE_NO_READBACK)) {
-        kappa::launch_to_f32(stream_, k, A.nfine);
+        // e = (float)x64 for every island, written to mapped callers' phi in the same launch
+        kappa::launch_arena_readback(stream_, A.d_io, (int)set.size(), A.io_blocks, k.x64, k.e);
         launches_++;
         nl++;
         for (size_t q = 0; q < set.size(); q++) {
+            if (A.io[q].h_phi_out) continue;
             const Island* s = set[q];
             if (!CU_OK(cudaMemcpyAsync(s->hosts.k_phi, k.e + A.desc[q].off, (size_t)s->n * 4, cudaMemcpyDeviceToHost,
                                        stream_)))

@@ -230,18 +230,6 @@ __global__ void k_ctl_finish(const __grid_constant__ KArena A, int isl, const Pl
 
 }  // namespace
 
-namespace {
-__global__ void k_to_f32(const double* __restrict__ x, float* __restrict__ out, int64_t n) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = (float)x[i];
-}
-}  // namespace
-
-// phi (FP32) = x64 rounded, staged in a.e for the copy back to the host
-void launch_to_f32(cudaStream_t s, const KArena& a, int64_t n) {
-    k_to_f32<<<(unsigned)ceil_div64(n, 256), 256, 0, s>>>(a.x64, a.e, n);
-}
-
 // Coarsen by 2 per axis until a level has at most 64 cells (or a side of 2,
 // or kMaxLevels levels).
 int plan_levels(int lx, int ly, int lz, KLevel* lev) {

@@ -185,6 +185,10 @@ PFSF_API void pfsf_set_mg_cycle(pfsf_engine e, pfsf_mg_cycle cycle) {
     if (Engine* g = E(e)) g->set_mg_cycle((int)cycle);
 }
 
+PFSF_API void pfsf_set_amg(pfsf_engine e, int32_t enable) {
+    if (Engine* g = E(e)) g->set_amg(enable != 0);
+}
+
 PFSF_API pfsf_result pfsf_get_tuning(pfsf_engine e, pfsf_tuning* out) {
     Engine* g = E(e);
     return g ? g->get_tuning(out) : PFSF_ERROR_INVALID_ARG;

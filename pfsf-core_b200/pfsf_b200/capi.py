@@ -179,6 +179,7 @@ def load():
         "pfsf_island_phi_max": ([E, C.c_int32, C.POINTER(C.c_float)], C.c_int),
         "pfsf_get_tuning": ([E, C.POINTER(Tuning)], C.c_int),
         "pfsf_set_mg_cycle": ([E, C.c_int], None),
+        "pfsf_set_amg": ([E, C.c_int32], None),
         "pfsf_debug_time_pass": ([E, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_double)],
                                  C.c_int),
         "pfsf_set_tuning": ([E, C.POINTER(Tuning)], C.c_int),
@@ -346,12 +347,14 @@ class Engine:
         return rc, out[:cnt.value]
 
     FIELD_DTYPES = {0: np.float32, 1: np.float32, 2: np.float32, 3: np.uint8, 4: np.uint32, 6: np.float32,
-                    7: np.float32, 8: np.uint8, 9: np.float32, 10: np.float32, 11: np.float32}
+                    7: np.float32, 8: np.uint8, 9: np.float32, 10: np.float32, 11: np.float32, 12: np.int32,
+                    13: np.float32, 14: np.float32}
 
     def debug_field(self, iid, field):
         """Tick-state array of an island (0 phi, 1 H, 2 d, 3 fail, 4 macro bits,
         6 source, 7 face conductivity SoA-6, 8 type, 9 max_phi, 10 rcomp,
-        11 rtens) or the schedule state dict (field 5)."""
+        11 rtens, 12 aggregates, 13 aggregation weights, 14 coarse diagonal)
+        or the schedule state dict (field 5)."""
         size = C.c_int64(0)
         tmp = np.zeros(32, np.uint8)
         rc = self.L.pfsf_debug_read_field(self.h, iid, field, _ptr(tmp), 0, C.byref(size))
@@ -390,6 +393,10 @@ class Engine:
     def set_mg_cycle(self, cycle):
         """MG_V (0) or MG_W (1) for the batched tolerance solve's preconditioner."""
         self.L.pfsf_set_mg_cycle(self.h, int(cycle))
+
+    def set_amg(self, on):
+        """Aggregation correction at every PCG start of the reference tick."""
+        self.L.pfsf_set_amg(self.h, int(bool(on)))
 
     def set_pcg_enabled(self, on):
         self.L.pfsf_set_pcg_enabled(self.h, int(bool(on)))

@@ -300,3 +300,48 @@ def test_sparse_scatter_updates_device_arrays(eng):
         fb, want = _tick_both(eng, iid, host, ref, origin)
         _assert_tick_parity(eng, iid, host, ref, fb, want, t)
         eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+
+
+def test_amg_correction_matches_oracle(eng):
+    """pfsf_set_amg: every PCG start applies the aggregation correction
+    (NP/src/solver/dispatcher_amg.cpp:83-161 with the aggregates of
+    amg_builder.cpp:9-63).  Two islands ticked together in one batched tick
+    until PCG engages; after every tick the state agrees with oracle islands
+    that run the same correction, and the device-built aggregates, weights
+    and coarse diagonal equal the oracle builder's bit for bit (the oracle
+    builder is itself bit-exact against the reference's, test_amg_oracle.py)."""
+    eng.set_amg(True)
+    try:
+        origins = [(0, 0, 0), (40, 1, -3)]
+        setups = []
+        for name, origin in zip(("block16", "noise20"), origins):
+            case = cases.compat_case(name)
+            iid, host, _ = _setup(eng, case, origin)
+            ref = O.Island(*case["dims"], amg=True)
+            ref.load(phi=case["phi"], source=case["source"], conductivity=case["conductivity"], type=case["type"],
+                     rcomp=case["rcomp"], rtens=case["rtens"], max_phi=case["max_phi"],
+                     hydration=case["hydration"])
+            setups.append((iid, host, ref, case))
+        built = False
+        for t in range(8):
+            for iid, _, _, _ in setups:
+                eng.L.pfsf_mark_full_rebuild(eng.h, iid)
+            fb = np.zeros(1 + 4 * 8192, np.int32)
+            assert eng.tick_dbb([s[0] for s in setups], fb) == capi.PFSF_OK
+            want_count = 0
+            for (iid, host, ref, case), origin in zip(setups, origins):
+                ref.tick()
+                want_count += int(ref.failures(origin, capacity=8192)[0])
+                _assert_island_state(eng, iid, host, ref, t)
+                if ref.state()["pcg_allocated"] == 1:
+                    agg, w, dc = O.amg_build(case["dims"], case["conductivity"], case["type"])
+                    g_agg = eng.debug_field(iid, 12)
+                    if g_agg.size:
+                        built = True
+                        assert np.array_equal(g_agg, agg), f"tick {t}: aggregates"
+                        assert np.array_equal(eng.debug_field(iid, 13).view(np.uint32), w.view(np.uint32))
+                        assert np.array_equal(eng.debug_field(iid, 14).view(np.uint32), dc.view(np.uint32))
+            assert fb[0] == want_count, f"tick {t}: failure count"
+        assert built, "PCG (and with it the correction) never engaged"
+    finally:
+        eng.set_amg(False)
