@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--island-report", default="",
                     help="write one JSON line per island of the last timed solve (team, iterations, times)")
     ap.add_argument("--precision", choices=["bf16", "fp16", "fp32"], default="bf16")
-    ap.add_argument("--cycle", choices=["v", "w"], default="w",
-                    help="fracture workload: multigrid cycle of the batched solve (the configuration asks for W)")
+    ap.add_argument("--cycle", choices=["v", "w"], default=None,
+                    help="multigrid cycle of the batched solve: default W for the fracture workload (the "
+                         "configuration asks for W), V otherwise")
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
@@ -109,7 +110,7 @@ def write_island_report(path, eng, ids, isls):
                                 "inner": r.inner_iterations, "outer": r.outer_iterations,
                                 "converged": r.converged, "rel_residual": r.rel_residual,
                                 "solve_ms": r.solve_ms, "setup_ms": r.setup_ms,
-                                "precond_ms": r.precond_ms}) + "\n")
+                                "precond_ms": r.precond_ms, "start_ms": r.start_ms}) + "\n")
 
 
 def stratified(isls, k):
@@ -344,6 +345,7 @@ def run_ours(args):
     mode = capi.SOLVE_BATCHED
     eng.set_solve_mode(mode)
     eng.set_precision(prec)
+    eng.set_mg_cycle(capi.MG_W if args.cycle == "w" else capi.MG_V)
     rc, st0 = eng.solve(ids, tol=args.tol, flags=capi.SOLVE_COLD_START)  # builds and uploads the arena
     assert rc == capi.PFSF_OK
     resident = capi.SOLVE_NO_UPLOAD | capi.SOLVE_NO_READBACK | capi.SOLVE_COLD_START
@@ -499,6 +501,7 @@ def run_ours(args):
                                            "tail": stats[-1].vcycle_tail_ms_sum},
                          "persistent_ctas": stats[-1].persistent_ctas,
                          "tuning": tuning,
+                         "cycle": "W" if args.cycle == "w" else "V",
                          "smoother": os.environ.get("PFSF_SMOOTHER", "chebyshev(batched)")},
         }
         print(json.dumps(line), flush=True)
@@ -640,7 +643,7 @@ def run_fracture(args):
         assert eng.register_kappa(iid, phik, src, isl.kappa, isl.vtype) == capi.PFSF_OK
         eng.set_solve_mode(mode)
         eng.set_precision(prec)
-        eng.set_mg_cycle(capi.MG_W if args.cycle == "w" else capi.MG_V)
+        eng.set_mg_cycle(capi.MG_V if args.cycle == "v" else capi.MG_W)
         if scale is None:  # loads scaled so max phi = 20 at 1x: the phase field and the scan act
             rc, st = eng.solve([iid], tol=1e-6, flags=capi.SOLVE_COLD_START)
             scale = 20.0 / float(np.abs(phik).max())
@@ -682,7 +685,7 @@ def run_fracture(args):
                                f"component), {args.ticks} ticks, load ramped 1x->2x, warm start",
                    "grid_voxels": n, "active_voxels": int(isl.n_active), "precision": args.precision,
                    "tol": args.tol, "generation_s": t_gen,
-                   "cycle": ("W" if args.cycle == "w" else "V") + "-cycle preconditioner (batched solve; the plain "
+                   "cycle": ("V" if args.cycle == "v" else "W") + "-cycle preconditioner (batched solve; the plain "
                             "per-island solve runs V-cycles)"},
         "solve_device_ms_mean": float(np.mean(m["dev"])), "inner_iterations_mean": float(np.mean(m["iters"])),
         "max_rel_residual_fp64": m["relres"], "failures_last_tick": m["fails"][-1],

@@ -148,6 +148,7 @@ typedef struct pfsf_island_report {
     double solve_ms;           /* batched mode: the island's solve time */
     double setup_ms;           /* batched mode: hierarchy build */
     double precond_ms;         /* batched mode: time in V-cycles */
+    double start_ms;           /* batched mode: solve start after the first island's start */
 } pfsf_island_report;
 
 PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine engine, int32_t island_id, pfsf_island_report* out);

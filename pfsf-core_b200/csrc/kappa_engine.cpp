@@ -633,6 +633,10 @@ pfsf_result Engine::island_report(int32_t id, pfsf_island_report* out) const {
         r.solve_ms = (double)(d.t_end - d.t_start) * 1e-6;
         r.setup_ms = (double)d.t_setup * 1e-6;
         r.precond_ms = (double)d.t_precond * 1e-6;
+        unsigned long long t0 = d.t_start;
+        for (const KDesc& o : arena_->desc)
+            if (o.team != PFSF_TEAM_PLAIN && o.t_start > 0) t0 = std::min(t0, o.t_start);
+        r.start_ms = (double)(d.t_start - t0) * 1e-6;
     }
     *out = r;
     return PFSF_OK;

@@ -97,7 +97,7 @@ class IslandReport(C.Structure):
                 ("levels", C.c_int32), ("inner_iterations", C.c_int32), ("outer_iterations", C.c_int32),
                 ("converged", C.c_int32), ("team", C.c_int32), ("team_ctas", C.c_int32),
                 ("rel_residual", C.c_double), ("solve_ms", C.c_double), ("setup_ms", C.c_double),
-                ("precond_ms", C.c_double)]
+                ("precond_ms", C.c_double), ("start_ms", C.c_double)]
 
 
 class TickReport(C.Structure):
