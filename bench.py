@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--cycle", choices=["v", "w"], default=None,
                     help="multigrid cycle of the batched solve: default W for the fracture workload (the "
                          "configuration asks for W), V otherwise")
+    ap.add_argument("--amg", action="store_true",
+                    help="tick_dbb workload: the aggregation correction at every PCG start (pfsf_set_amg)")
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
@@ -732,6 +734,7 @@ def run_tick_dbb(args):
     eng = capi.Engine(capi.default_config(max_island_size=1 << 28, tick_budget_ms=1 << 30, vram=180 << 30))
     if eng.init() != capi.PFSF_OK:
         raise RuntimeError("pfsf_init failed")
+    eng.set_amg(args.amg)
     ids = []
     for k, (isl, h) in enumerate(zip(isls, host)):
         iid = k + 1
@@ -771,7 +774,9 @@ def run_tick_dbb(args):
         "data": "synthetic", "dtype": "f32",
         "config": {"workload": (f"{len(isls)} islands (log-uniform sides, scale {meta['scale']:.3f}), "
                                 f"{meta['grid_total']} grid / {meta['active_total']} active voxels, all dirty every "
-                                f"tick, 16-step reference schedule"), "islands": len(isls),
+                                f"tick, 16-step reference schedule"
+                                + (", aggregation correction at every PCG start" if args.amg else "")),
+                   "islands": len(isls),
                    "grid_voxels": meta["grid_total"], "active_voxels": meta["active_total"],
                    "generation_s": t_gen},
         "e2e": {"value": float(np.mean(walls)), "unit": "ms/tick", "h2d_bytes_per_step": int(h2d),
@@ -785,6 +790,7 @@ def run_tick_dbb(args):
         "gpu_launches": int(np.mean([r.kernel_launches for r in reps])),
         "groups": int(reps[-1].groups), "graph_replayed": int(reps[-1].graph_replayed),
         "failures_last_tick": int(fb[0]), "clocks": clk.summary(),
+        "macro_residual_max": float(max(eng.debug_field(i, 5)["last_macro"] for i in ids)),
     }
     print(json.dumps(line), flush=True)
     eng.close()

@@ -32,9 +32,14 @@ namespace {
 
 // 512 threads, two CTAs (two islands) per SM: the passes are latency bound
 // (L2 round trips between CTA barriers), so warps per SM matter more than
-// registers per thread (measured: 256 x 2 with 128 registers took 1.8x longer).
+// registers per thread (measured: 256 x 2 with 128 registers took 1.8x longer),
+// but not at any price in spills (3 CTAs per SM at 40 registers, with twice
+// the spill traffic, took 11 % longer on the 4096-island solve).
+#ifndef PFSF_BATCHED_MIN_BLOCKS
+#define PFSF_BATCHED_MIN_BLOCKS 2
+#endif
 constexpr int kBatchedThreads = 512;
-constexpr int kBatchedMinBlocks = 2;
+constexpr int kBatchedMinBlocks = PFSF_BATCHED_MIN_BLOCKS;
 static_assert(kBatchedThreads == kFlatThreads, "the tile marching passes assume one CTA of kFlatThreads");
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -712,26 +717,32 @@ cudaError_t launch_one(cudaStream_t s, const KArena& a, int base, int nbig, int 
 // clustered launch leaves free get a second, cluster-less launch on the
 // side stream: it takes CTA- and warp-sized islands from the same queues
 // from the start.  Neither launch waits on the other (islands are handed
-// out by atomic counters), so they need not run at the same time.
+// out by atomic counters), so they need not run at the same time; the fork
+// is recorded before the clustered launch, so that the side launch depends
+// only on the work before both (recorded after it, the side launch would
+// wait for the clustered kernel to finish and find the queues empty).
 template <int P, int C>
 cudaError_t launch_clustered(cudaStream_t s, const SideStream& side, const KArena& a, int base, int nbig,
                              int nsmall, int num_sms, int* ctas, int* launches) {
+    const int nmid = a.nisl - base - nbig - nsmall;
+    const bool fork = side.stream && nmid + nsmall > 0;
+    if (fork &&
+        (cudaEventRecord(side.fork, s) != cudaSuccess || cudaStreamWaitEvent(side.stream, side.fork, 0) != cudaSuccess))
+        return cudaErrorLaunchFailure;
     int used = 0, slots = 0;
     cudaError_t e = launch_one<P, C>(s, a, base, nbig, nsmall, num_sms, 0, &used, &slots);
     if (e != cudaSuccess) return e;
     *ctas = used;
     *launches = 1;
-    const int nmid = a.nisl - base - nbig - nsmall;
-    if (slots > used && side.stream && nmid + nsmall > 0) {
+    if (fork) {
         int used2 = 0, slots2 = 0;
-        if (cudaEventRecord(side.fork, s) != cudaSuccess || cudaStreamWaitEvent(side.stream, side.fork, 0) != cudaSuccess)
-            return cudaErrorLaunchFailure;
-        e = launch_one<P, 1>(side.stream, a, base, nbig, nsmall, num_sms, slots - used, &used2, &slots2);
+        if (slots > used)
+            e = launch_one<P, 1>(side.stream, a, base, nbig, nsmall, num_sms, slots - used, &used2, &slots2);
         if (e != cudaSuccess) return e;
         if (cudaEventRecord(side.join, side.stream) != cudaSuccess || cudaStreamWaitEvent(s, side.join, 0) != cudaSuccess)
             return cudaErrorLaunchFailure;
         *ctas += used2;
-        *launches += 1;
+        *launches += used2 > 0 ? 1 : 0;
     }
     return cudaSuccess;
 }
