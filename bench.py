@@ -789,6 +789,9 @@ def run_tick_dbb(args):
         "voxel_updates_per_s": 16.0 * meta["grid_total"] / (dev_ms * 1e-3),
         "gpu_launches": int(np.mean([r.kernel_launches for r in reps])),
         "groups": int(reps[-1].groups), "graph_replayed": int(reps[-1].graph_replayed),
+        "graph_use": {"replayed": sum(r.graph_replayed == 1 for r in reps),
+                      "updated": sum(r.graph_replayed == 2 for r in reps),
+                      "instantiated": sum(r.graph_replayed == 0 for r in reps)},
         "failures_last_tick": int(fb[0]), "clocks": clk.summary(),
         "macro_residual_max": float(max(eng.debug_field(i, 5)["last_macro"] for i in ids)),
     }

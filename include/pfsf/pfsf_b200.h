@@ -159,8 +159,8 @@ PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine engine, int32_t island
  * island set, one section per GPU model and SM count) -- the file named by
  * PFSF_TUNE_FILE, else tune/pfsf_tune.txt beside the library's lib/
  * directory -- then from the PFSF_CLUSTER, PFSF_CLUSTER_MIN_VOXELS,
- * PFSF_GRID_MIN_VOXELS, PFSF_WARP_MAX_VOXELS, PFSF_CHEB_K variables when set;
- * built-in defaults otherwise. */
+ * PFSF_GRID_MIN_VOXELS, PFSF_WARP_MAX_VOXELS, PFSF_CHEB_K, PFSF_CHEB_LOWER,
+ * PFSF_COARSE_WEIGHT variables when set; built-in defaults otherwise. */
 typedef enum pfsf_tuning_source {
     PFSF_TUNING_DEFAULT = 0,  /* built-in defaults */
     PFSF_TUNING_FILE = 1,     /* the tuning file's section for this GPU */
@@ -176,6 +176,9 @@ typedef struct pfsf_tuning {
     int64_t warp_max_voxels;      /* islands below this many voxels go to single warps (0: none) */
     int32_t cheb_k;               /* Chebyshev smoothing degree, 1..4 */
     int32_t source;               /* pfsf_tuning_source (read only) */
+    /* solver parameters (read and written only when struct_bytes covers them) */
+    float cheb_lower;             /* Chebyshev interval [cheb_lower * lmax, lmax], 0 < cheb_lower < 1 */
+    float coarse_weight;          /* coarse-correction weight of the V-cycle, 0 < w < 2 (keeps it SPD) */
 } pfsf_tuning;
 
 PFSF_API pfsf_result pfsf_get_tuning(pfsf_engine engine, pfsf_tuning* out);
@@ -191,7 +194,8 @@ typedef struct pfsf_tick_report {
     int32_t struct_bytes;
     int32_t islands;           /* islands dispatched */
     int32_t groups;            /* schedule groups */
-    int32_t graph_replayed;    /* 1: the captured launch sequence was reused */
+    int32_t graph_replayed;    /* 1: the captured launch sequence was reused; 2: captured again and the
+                                  instantiated graph updated in place; 0: captured and instantiated */
     int64_t kernel_launches;   /* kernels the tick launched */
     double algorithmic_bytes;  /* device-memory bytes of the tick's passes: every
                                   array a pass touches counted once per pass */

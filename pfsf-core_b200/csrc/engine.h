@@ -262,6 +262,8 @@ private:
     int64_t warp_max_voxels_ = 0;         // PFSF_WARP_MAX_VOXELS (0: no warp tier)
     int smoother_ = -1;                   // PFSF_SMOOTHER (-1: mode default)
     int cheb_k_ = 3;                      // PFSF_CHEB_K
+    float cheb_lower_ = 0.1f;             // PFSF_CHEB_LOWER: Chebyshev interval [lower * lmax, lmax]
+    float coarse_weight_ = 1.8f;          // PFSF_COARSE_WEIGHT: V-cycle coarse-correction weight
     int tuning_source_ = PFSF_TUNING_DEFAULT;
     int mg_cycle_ = 0;                    // 0 V-cycle, 1 W-cycle (batched tolerance solve)
     void load_tuning();                   // tuning file, then environment overrides (init)

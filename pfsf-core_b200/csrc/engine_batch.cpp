@@ -110,6 +110,9 @@ void Engine::free_tick_batch() {
     if (B.ev0) cudaEventDestroy(B.ev0);
     if (B.ev1) cudaEventDestroy(B.ev1);
     if (B.exec) cudaGraphExecDestroy(B.exec);
+    for (cudaStream_t ls : B.lanes) cudaStreamDestroy(ls);
+    for (cudaEvent_t le : B.lane_done) cudaEventDestroy(le);
+    if (B.fork) cudaEventDestroy(B.fork);
     if (B.d_tab) cudaFree(B.d_tab);
     if (B.d_bs) cudaFree(B.d_bs);
     if (B.d_res) cudaFree(B.d_res);
@@ -332,34 +335,56 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
     }
     if (!ok) return PFSF_ERROR_VULKAN;
 
-    if (B.exec && B.key != key) {
-        cudaGraphExecDestroy(B.exec);
-        B.exec = nullptr;
-    }
-    const bool replayed = B.exec != nullptr;
-    if (!B.exec) {
+    // a tick of another structure is captured again; its graph then updates
+    // the instantiated one in place when the topology is the same (only
+    // launch shapes and arguments differ), else it is instantiated anew
+    const bool replayed = B.exec != nullptr && B.key == key;
+    bool updated = false;
+    if (!replayed) {
         // ---- record the tick once, under capture
         B.effects.assign(ng, TickEffect{});
         int64_t nl = 0;
         cudaGraph_t graph = nullptr;
+        // groups touch disjoint islands: each group's chain (its upload, macro
+        // seeding, schedule) is a branch of its own, on one of up to kLanes
+        // capture streams, so small groups run beside big ones and a group's
+        // sweeps start as soon as its own arrays are in; the tail over all
+        // islands joins them.
+        const int lanes = tail_only ? 0 : std::min(ng, kLanes);
+        for (int l = (int)B.lanes.size(); l < lanes; l++) {
+            cudaStream_t ls = nullptr;
+            cudaEvent_t le = nullptr;
+            if (!CU_OK(cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking)) ||
+                !CU_OK(cudaEventCreateWithFlags(&le, cudaEventDisableTiming)))
+                return PFSF_ERROR_VULKAN;
+            B.lanes.push_back(ls);
+            B.lane_done.push_back(le);
+        }
+        if (lanes > 0 && !B.fork &&
+            !CU_OK(cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming)))
+            return PFSF_ERROR_VULKAN;
         if (!CU_OK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal))) return PFSF_ERROR_VULKAN;
-        const cudaStream_t st = stream_;
-        compat::batch::upload(st, ALL);
-        nl++;
+        cudaStream_t st = stream_;
+        bool fork_ok = true;
+        if (lanes > 0) {
+            fork_ok &= CU_OK(cudaEventRecord(B.fork, stream_));
+            for (int l = 0; l < lanes; l++) fork_ok &= CU_OK(cudaStreamWaitEvent(B.lanes[l], B.fork, 0));
+        }
         if (tail_only) {
+            compat::batch::upload(st, ALL);
             // the solved phi (the history update below is the one the
             // reference performs inside its sweeps, rbgs_smooth.comp.glsl:177-191)
             compat::batch::take_phi(st, ALL);
-            nl++;
-        }
-        compat::batch::macro_fill(st, ALL);
-        nl++;
-        if (tail_only) {
+            compat::batch::macro_fill(st, ALL);
             compat::batch::history(st, ALL);
-            nl++;
+            nl += 4;
         }
         for (int q = 0; q < ng && !tail_only; q++) {
             const compat::BGroup& g = G[q];
+            st = B.lanes[q % lanes];
+            compat::batch::upload(st, g);
+            compat::batch::macro_fill(st, g);
+            nl += 2;
             const Plan& p = plan[order[groups[q].first]];
             TickEffect& ef = B.effects[q];
             auto rbgs_step = [&](int sidx_damp) {
@@ -444,6 +469,11 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
                 }
             }
         }
+        st = stream_;
+        for (int l = 0; l < lanes; l++) {
+            fork_ok &= CU_OK(cudaEventRecord(B.lane_done[l], B.lanes[l]));
+            fork_ok &= CU_OK(cudaStreamWaitEvent(stream_, B.lane_done[l], 0));
+        }
         // the tick's tail over every island (pfsf_engine.cpp:513-560)
         if (cfg_.enable_phase_field) {
             compat::batch::copy_damage(st, ALL);
@@ -459,12 +489,23 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
         compat::batch::stress_out(st, ALL);
         nl++;
         const cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
-        if (ce != cudaSuccess || !graph) {
+        if (ce != cudaSuccess || !graph || !fork_ok) {
+            if (graph) cudaGraphDestroy(graph);
             std::fprintf(stderr, "[libpfsf] tick capture failed: %s\n", cudaGetErrorString(ce));
             cudaGetLastError();
             return PFSF_ERROR_VULKAN;
         }
-        const cudaError_t ie = cudaGraphInstantiate(&B.exec, graph, 0);
+        if (B.exec) {
+            cudaGraphExecUpdateResultInfo info{};
+            if (cudaGraphExecUpdate(B.exec, graph, &info) == cudaSuccess) {
+                updated = true;
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(B.exec);
+                B.exec = nullptr;
+            }
+        }
+        const cudaError_t ie = updated ? cudaSuccess : cudaGraphInstantiate(&B.exec, graph, 0);
         cudaGraphDestroy(graph);
         if (ie != cudaSuccess) {
             std::fprintf(stderr, "[libpfsf] tick graph instantiation failed: %s\n", cudaGetErrorString(ie));
@@ -494,7 +535,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
     R.struct_bytes = (int32_t)sizeof(R);
     R.islands = nisl;
     R.groups = tail_only ? 1 : ng;
-    R.graph_replayed = replayed ? 1 : 0;
+    R.graph_replayed = replayed ? 1 : (updated ? 2 : 0);
     R.kernel_launches = B.graph_launches;
     for (int j = 0; j < nisl; j++) {
         const Island& s = *set[order[j]];

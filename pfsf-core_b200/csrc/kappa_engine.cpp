@@ -274,7 +274,7 @@ KArena Engine::solve_params(double tol, int32_t max_iter) const {
     k.eta_min = 1e-4;
     k.max_outer = 8;
     k.max_inner = max_iter > 0 ? max_iter : 500;
-    k.omega_c = 1.8f;
+    k.omega_c = coarse_weight_;
     k.nu = 2;
     k.coarse_sweeps = 4;
     const bool batched = solve_mode_ == PFSF_SOLVE_BATCHED;
@@ -285,7 +285,7 @@ KArena Engine::solve_params(double tol, int32_t max_iter) const {
     k.wcycle = (batched && mg_cycle_ == 1) ? 1 : 0;
     k.cheb_k = std::max(1, std::min(4, cheb_k_));
     {
-        const double lmax = 2.0, lmin = lmax * 0.1;
+        const double lmax = 2.0, lmin = lmax * (double)cheb_lower_;
         const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
         double rho = 1.0 / sigma;
         k.cheb_c1[0] = 0.0f;
@@ -343,7 +343,8 @@ pfsf_result Engine::run_solve(const KArena& k, int64_t& nl) {
     const std::vector<double> key = {k.tol, k.eta_min, (double)k.max_inner, (double)k.max_outer, (double)k.omega_c,
                                      (double)k.nu, (double)k.coarse_sweeps, (double)k.fp64_dots, (double)k.smoother,
                                      (double)k.cheb_k, (double)k.wcycle, (double)k.prec, (double)nbig, (double)nsmall,
-                                     (double)cluster_size_, (double)num_sms_, (double)nisl};
+                                     (double)cluster_size_, (double)num_sms_, (double)nisl, (double)k.cheb_c2[0],
+                                     (double)k.cheb_c1[1]};
     *flag = 0;
     if (ngiant == 0 && A.launched && !A.graph_off) {
         if (A.solve_exec && A.solve_key != key) {

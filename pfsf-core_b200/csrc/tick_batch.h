@@ -32,6 +32,13 @@ struct Engine::TickBatch {
     bool have_tick = false;
     pfsf_tick_report last{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // capture streams of the groups' branches, their join events, the fork
+    std::vector<cudaStream_t> lanes;
+    std::vector<cudaEvent_t> lane_done;
+    cudaEvent_t fork = nullptr;
 };
+
+// group branches of one captured tick
+constexpr int kLanes = 8;
 
 }  // namespace pfsf_b200

@@ -1,6 +1,6 @@
-// Launch-shape parameters of the batched tolerance solve: the tuning file
-// written by the autotuner (pfsf_b200/autotune.py), environment overrides,
-// and the pfsf_get_tuning / pfsf_set_tuning exports.
+// Launch-shape and smoother parameters of the batched tolerance solve: the
+// tuning file written by the autotuner (pfsf_b200/autotune.py), environment
+// overrides, and the pfsf_get_tuning / pfsf_set_tuning exports.
 //
 // File format (text): '#' comments, one section per GPU model,
 //     [<device name> <SM count>]
@@ -10,6 +10,7 @@
 // The engine takes the section whose name and SM count match its device.
 #include <dlfcn.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -29,9 +30,15 @@ std::string trim(const std::string& s) {
     return s.substr(a, b - a + 1);
 }
 
+// the solver parameters are part of a caller's struct only when its size covers them
+bool has_solver(const pfsf_tuning& t) { return t.struct_bytes >= (int32_t)sizeof(pfsf_tuning); }
+
 bool valid(const pfsf_tuning& t) {
-    return (t.cluster == 1 || t.cluster == 4 || t.cluster == 8) && t.cluster_min_voxels >= 0 &&
-           t.grid_min_voxels >= 0 && t.warp_max_voxels >= 0 && t.cheb_k >= 1 && t.cheb_k <= 4;
+    const bool launch = (t.cluster == 1 || t.cluster == 4 || t.cluster == 8) && t.cluster_min_voxels >= 0 &&
+                        t.grid_min_voxels >= 0 && t.warp_max_voxels >= 0 && t.cheb_k >= 1 && t.cheb_k <= 4;
+    const bool solver = !has_solver(t) || (t.cheb_lower > 0.0f && t.cheb_lower < 1.0f && t.coarse_weight > 0.0f &&
+                                           t.coarse_weight < 2.0f);
+    return launch && solver;
 }
 
 // tune/pfsf_tune.txt beside the directory that holds this library
@@ -81,6 +88,8 @@ void Engine::load_tuning() {
         else if (k == "grid_min_voxels") t.grid_min_voxels = v;
         else if (k == "warp_max_voxels") t.warp_max_voxels = v;
         else if (k == "cheb_k") t.cheb_k = (int32_t)v;
+        else if (k == "cheb_lower") t.cheb_lower = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
+        else if (k == "coarse_weight") t.coarse_weight = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
     }
     if (found && valid(t)) {
         set_tuning(&t);
@@ -95,6 +104,8 @@ void Engine::load_tuning() {
     if (const char* f = std::getenv("PFSF_CLUSTER")) { cluster_size_ = std::atoi(f); over = true; }
     if (const char* f = std::getenv("PFSF_WARP_MAX_VOXELS")) { warp_max_voxels_ = std::atoll(f); over = true; }
     if (const char* f = std::getenv("PFSF_CHEB_K")) { cheb_k_ = std::atoi(f); over = true; }
+    if (const char* f = std::getenv("PFSF_CHEB_LOWER")) { cheb_lower_ = std::strtof(f, nullptr); over = true; }
+    if (const char* f = std::getenv("PFSF_COARSE_WEIGHT")) { coarse_weight_ = std::strtof(f, nullptr); over = true; }
     if (over) tuning_source_ = PFSF_TUNING_ENV;
 }
 
@@ -108,7 +119,11 @@ pfsf_result Engine::get_tuning(pfsf_tuning* out) const {
     t.warp_max_voxels = warp_max_voxels_;
     t.cheb_k = cheb_k_;
     t.source = tuning_source_;
-    *out = t;
+    t.cheb_lower = cheb_lower_;
+    t.coarse_weight = coarse_weight_;
+    // a caller's older, shorter struct gets the fields it has
+    const size_t n = out->struct_bytes > 0 ? std::min(sizeof(t), (size_t)out->struct_bytes) : sizeof(t);
+    std::memcpy(out, &t, n);
     return PFSF_OK;
 }
 
@@ -119,6 +134,10 @@ pfsf_result Engine::set_tuning(const pfsf_tuning* in) {
     grid_min_voxels_ = in->grid_min_voxels;
     warp_max_voxels_ = in->warp_max_voxels;
     cheb_k_ = in->cheb_k;
+    if (has_solver(*in)) {
+        cheb_lower_ = in->cheb_lower;
+        coarse_weight_ = in->coarse_weight;
+    }
     tuning_source_ = PFSF_TUNING_CALLER;
     return PFSF_OK;
 }

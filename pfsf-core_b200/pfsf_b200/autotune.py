@@ -5,7 +5,8 @@
 Parameters tuned (pfsf_tuning, include/pfsf/pfsf_b200.h): the cluster size
 for big islands (1, 4, 8 CTAs), the island size from which clusters take
 over from single CTAs, the size below which single warps take islands, the
-Chebyshev smoothing degree, and the size from which one island takes the
+Chebyshev smoothing degree and the lower end of its interval, the V-cycle's
+coarse-correction weight, and the size from which one island takes the
 whole GPU.  Method: timed trials -- the device time of a resident solve to
 the benchmark tolerance (median of `reps`) -- by coordinate descent from the
 current values, on a size-bucketed island set drawn like the benchmark's
@@ -27,12 +28,16 @@ import numpy as np
 from . import capi, synth
 
 DEFAULT_FILE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tune", "pfsf_tune.txt")
-KEYS = ("cluster", "cluster_min_voxels", "grid_min_voxels", "warp_max_voxels", "cheb_k")
+KEYS = ("cluster", "cluster_min_voxels", "grid_min_voxels", "warp_max_voxels", "cheb_k", "cheb_lower",
+        "coarse_weight")
+FLOAT_KEYS = ("cheb_lower", "coarse_weight")
 CANDIDATES = {
     "cluster": [1, 4, 8],
     "cluster_min_voxels": [32768, 65536, 131072, 262144, 524288],
     "warp_max_voxels": [0, 1024, 2048],
     "cheb_k": [2, 3, 4],
+    "cheb_lower": [0.05, 0.1, 0.15, 0.2, 0.3],
+    "coarse_weight": [1.0, 1.4, 1.6, 1.8, 1.9],
 }
 
 
@@ -78,7 +83,7 @@ def tune(eng, islands=4096, target_active=6.0e7, big_dims=(160, 160, 96), tol=1e
     t_end = time.monotonic() + budget_s
     trials = []
     rc, t0 = eng.tuning()
-    best = {k: getattr(t0, k) for k in KEYS}
+    best = {k: (round(float(getattr(t0, k)), 6) if k in FLOAT_KEYS else getattr(t0, k)) for k in KEYS}
     eng.set_solve_mode(capi.SOLVE_BATCHED)
     eng.set_precision(capi.PREC_BF16)
     isls, _ = synth.batch(islands, seed=seed, target_active=target_active)
@@ -95,7 +100,7 @@ def tune(eng, islands=4096, target_active=6.0e7, big_dims=(160, 160, 96), tol=1e
         return ms
 
     best_ms = trial(best)
-    for key in ("cluster", "cluster_min_voxels", "cheb_k", "warp_max_voxels"):
+    for key in ("cluster", "cluster_min_voxels", "cheb_k", "cheb_lower", "coarse_weight", "warp_max_voxels"):
         for v in cands.get(key, []):
             if time.monotonic() > t_end:
                 break
@@ -154,7 +159,8 @@ def write_section(path, key, params, note=""):
     if note:
         out.append(f"# {note}")
     for k in KEYS:
-        out.append(f"{k} = {int(params[k])}")
+        if k in params:
+            out.append(f"{k} = {float(params[k]):g}" if k in FLOAT_KEYS else f"{k} = {int(params[k])}")
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
     with open(path, "w") as f:
         f.write("\n".join(out) + "\n")

@@ -113,12 +113,14 @@ class Tuning(C.Structure):
     SOURCES = {0: "default", 1: "file", 2: "env", 3: "caller"}
     _fields_ = [("struct_bytes", C.c_int32), ("cluster", C.c_int32), ("cluster_min_voxels", C.c_int64),
                 ("grid_min_voxels", C.c_int64), ("warp_max_voxels", C.c_int64), ("cheb_k", C.c_int32),
-                ("source", C.c_int32)]
+                ("source", C.c_int32), ("cheb_lower", C.c_float), ("coarse_weight", C.c_float)]
 
     def as_dict(self):
         return {"cluster": self.cluster, "cluster_min_voxels": self.cluster_min_voxels,
                 "grid_min_voxels": self.grid_min_voxels, "warp_max_voxels": self.warp_max_voxels,
-                "cheb_k": self.cheb_k, "source": self.SOURCES.get(self.source, str(self.source))}
+                "cheb_k": self.cheb_k, "cheb_lower": round(float(self.cheb_lower), 6),
+                "coarse_weight": round(float(self.coarse_weight), 6),
+                "source": self.SOURCES.get(self.source, str(self.source))}
 
 
 _lib = None
@@ -317,6 +319,7 @@ class Engine:
 
     def tuning(self):
         t = Tuning()
+        t.struct_bytes = C.sizeof(Tuning)
         rc = self.L.pfsf_get_tuning(self.h, C.byref(t))
         return rc, t
 
@@ -324,7 +327,7 @@ class Engine:
         """pfsf_set_tuning with the current values updated by kw."""
         rc, t = self.tuning()
         for k, v in kw.items():
-            setattr(t, k, int(v))
+            setattr(t, k, float(v) if k in ("cheb_lower", "coarse_weight") else int(v))
         t.struct_bytes = C.sizeof(Tuning)
         return self.L.pfsf_set_tuning(self.h, C.byref(t))
 

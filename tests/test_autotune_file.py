@@ -2,7 +2,8 @@
 place, read back by the same rules the engine uses (no GPU needed)."""
 from pfsf_b200 import autotune
 
-P = {"cluster": 4, "cluster_min_voxels": 262144, "grid_min_voxels": 2097152, "warp_max_voxels": 0, "cheb_k": 3}
+P = {"cluster": 4, "cluster_min_voxels": 262144, "grid_min_voxels": 2097152, "warp_max_voxels": 0, "cheb_k": 3,
+     "cheb_lower": 0.15, "coarse_weight": 1.6}
 
 
 def _read(path):
@@ -16,7 +17,7 @@ def _read(path):
             out[cur] = {}
             continue
         k, v = (x.strip() for x in s.split("=", 1))
-        out[cur][k] = int(v)
+        out[cur][k] = float(v) if k in autotune.FLOAT_KEYS else int(v)
     return out
 
 

@@ -10,7 +10,14 @@ from pfsf_b200 import autotune, capi
 
 pytestmark = pytest.mark.gpu
 
-ENV = ("PFSF_CLUSTER", "PFSF_CLUSTER_MIN_VOXELS", "PFSF_GRID_MIN_VOXELS", "PFSF_WARP_MAX_VOXELS", "PFSF_CHEB_K")
+ENV = ("PFSF_CLUSTER", "PFSF_CLUSTER_MIN_VOXELS", "PFSF_GRID_MIN_VOXELS", "PFSF_WARP_MAX_VOXELS", "PFSF_CHEB_K",
+       "PFSF_CHEB_LOWER", "PFSF_COARSE_WEIGHT")
+
+
+def _same(t, best):
+    """Engine values equal the tuner's (float parameters to FP32 rounding)."""
+    return all(abs(getattr(t, k) - best[k]) <= 1e-6 * max(1.0, abs(best[k])) if k in autotune.FLOAT_KEYS
+               else getattr(t, k) == best[k] for k in autotune.KEYS)
 
 
 def test_autotune_cache_is_read_at_init(lib_built, tmp_path, monkeypatch):
@@ -20,11 +27,11 @@ def test_autotune_cache_is_read_at_init(lib_built, tmp_path, monkeypatch):
     eng = capi.Engine(cfg)
     assert eng.init() == capi.PFSF_OK, "CUDA device required"
     best, trials = autotune.tune(eng, islands=48, target_active=3e5, big_dims=None, reps=1, budget_s=60.0,
-                                 candidates={"cluster": [1, 4], "cheb_k": [2, 3]})
+                                 candidates={"cluster": [1, 4], "cheb_k": [2, 3], "coarse_weight": [1.4, 1.8]})
     assert len(trials) >= 2 and np.isfinite(trials[0]["ms"])
     # the tuner leaves the winner set on its engine
     rc, t = eng.tuning()
-    assert rc == capi.PFSF_OK and all(getattr(t, k) == best[k] for k in autotune.KEYS)
+    assert rc == capi.PFSF_OK and _same(t, best)
     eng.close()
     path = tmp_path / "pfsf_tune.txt"
     key = autotune.device_key()
@@ -35,10 +42,12 @@ def test_autotune_cache_is_read_at_init(lib_built, tmp_path, monkeypatch):
     assert e2.init() == capi.PFSF_OK
     rc, t2 = e2.tuning()
     assert rc == capi.PFSF_OK and t2.source == 1, t2.as_dict()
-    assert all(getattr(t2, k) == best[k] for k in autotune.KEYS), (t2.as_dict(), best)
+    assert _same(t2, best), (t2.as_dict(), best)
     # out-of-range values are refused and change nothing
     assert e2.set_tuning(cluster=3) == capi.PFSF_ERROR_INVALID_ARG
     assert e2.set_tuning(cheb_k=0) == capi.PFSF_ERROR_INVALID_ARG
+    assert e2.set_tuning(coarse_weight=2.0) == capi.PFSF_ERROR_INVALID_ARG
+    assert e2.set_tuning(cheb_lower=0.0) == capi.PFSF_ERROR_INVALID_ARG
     rc, t3 = e2.tuning()
     assert t3.cluster == best["cluster"] and t3.cheb_k == best["cheb_k"]
     # an environment override wins over the file
