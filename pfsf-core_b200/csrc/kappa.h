@@ -96,6 +96,7 @@ struct KArena {
     int smoother;          // 0 symmetric 8-colour Gauss-Seidel, 1 Chebyshev
     int wcycle;            // 1: W-cycle (levels below level 1 visited twice), 0: V-cycle
     int cheb_k;            // polynomial degree (stencil passes per smoothing)
+    int tail_cells;        // coarse levels of at most this many cells run on one warp
     float cheb_c1[4], cheb_c2[4];
     // per island: solid voxels of each (tile, plane) as packed tile columns
     // (cx | cy << 16), island-relative at desc.off, and the table of list

@@ -262,7 +262,7 @@ __device__ __forceinline__ void t_copy(const KDesc& D, TeamT& tm, const float* s
     else op_copy((int)tm.t(), (int)tm.T(), (int)D.n, src, dst);
 }
 
-// One V-cycle z = M r.  Levels above kWarpTailCells cells are processed by
+// One V-cycle z = M r.  Levels above A.tail_cells cells are processed by
 // the whole team; from the first level at or below it the rest of the cycle
 // runs on one warp of the leader CTA (warp barriers only).
 template <int P, class TeamT>
@@ -277,7 +277,7 @@ __device__ void team_vcycle(const KArena& A, const KDesc& D, TeamT& tm) {
         return;
     }
     int l0 = 1;
-    while (l0 < L - 1 && D.lev[l0].n > kWarpTailCells) l0++;
+    while (l0 < L - 1 && D.lev[l0].n > A.tail_cells) l0++;
     for (int s = 0; s < A.nu; s++)
         for (int c = 0; c < 8; c++) { op_smooth0<P>(A, D, t, T, c); tm.sync(); }
     op_restrict0<P>(A, D, t, T);
@@ -288,7 +288,7 @@ __device__ void team_vcycle(const KArena& A, const KDesc& D, TeamT& tm) {
         op_restrictc<P>(A, D, l, t, T);
         tm.sync();
     }
-    if (D.lev[l0].n <= kWarpTailCells) {
+    if (D.lev[l0].n <= A.tail_cells) {
         if (tm.leader_warp()) warp_tail_vcycle<P>(A, D, l0, A.nu, A.coarse_sweeps, A.omega_c);
         tm.sync();
     } else {  // coarsest level still large: team sweeps
@@ -362,7 +362,7 @@ __device__ void team_chebc(const KArena& A, const KDesc& D, int l, TeamT& tm, bo
     }
 }
 
-// The rest of the V-cycle from coarse level l0 (<= kWarpTailCells cells) on
+// The rest of the V-cycle from coarse level l0 (<= A.tail_cells cells) on
 // one warp with Chebyshev smoothing: cheb_k passes per smoothing instead of
 // the 16 colour passes of two Gauss-Seidel sweeps, coarse_sweeps smoothings
 // on the coarsest level.
@@ -406,7 +406,7 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
         return;
     }
     int l0 = 1;
-    while (l0 < L - 1 && D.lev[l0].n > kWarpTailCells) l0++;
+    while (l0 < L - 1 && D.lev[l0].n > A.tail_cells) l0++;
     team_cheb0<P>(A, D, tm, true);
     t_restrict0<P>(A, D, tm);
     tm.sync();
@@ -419,7 +419,7 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
     }
     c0 = globaltimer();
     vt.coarse += c0 - c1;
-    if (D.lev[l0].n <= kWarpTailCells) {
+    if (D.lev[l0].n <= A.tail_cells) {
         if (tm.leader_warp()) warp_tail_cheb<P>(A, D, l0);
         tm.sync();
     } else {
@@ -449,7 +449,7 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
             op_restrictc<P>(A, D, l, t, T);
             tm.sync();
         }
-        if (D.lev[l0].n <= kWarpTailCells) {
+        if (D.lev[l0].n <= A.tail_cells) {
             if (tm.leader_warp()) warp_tail_cheb<P>(A, D, l0);
             tm.sync();
         } else {

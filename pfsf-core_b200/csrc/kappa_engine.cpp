@@ -284,6 +284,7 @@ KArena Engine::solve_params(double tol, int32_t max_iter) const {
     k.smoother = smoother_ >= 0 ? smoother_ : (batched ? 1 : 0);
     k.wcycle = (batched && mg_cycle_ == 1) ? 1 : 0;
     k.cheb_k = std::max(1, std::min(4, cheb_k_));
+    k.tail_cells = tail_cells_;
     {
         const double lmax = 2.0, lmin = lmax * (double)cheb_lower_;
         const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
@@ -344,7 +345,7 @@ pfsf_result Engine::run_solve(const KArena& k, int64_t& nl) {
                                      (double)k.nu, (double)k.coarse_sweeps, (double)k.fp64_dots, (double)k.smoother,
                                      (double)k.cheb_k, (double)k.wcycle, (double)k.prec, (double)nbig, (double)nsmall,
                                      (double)cluster_size_, (double)num_sms_, (double)nisl, (double)k.cheb_c2[0],
-                                     (double)k.cheb_c1[1]};
+                                     (double)k.cheb_c1[1], (double)k.tail_cells};
     *flag = 0;
     if (ngiant == 0 && A.launched && !A.graph_off) {
         if (A.solve_exec && A.solve_key != key) {

@@ -590,7 +590,7 @@ __device__ void op_chebc_dx(const KArena& A, const KDesc& D, int l, int t, int T
 // One warp runs the V-cycle from coarse level l0 down to the coarsest level
 // and back (pre-smoothing at l0 through post-smoothing at l0), with warp
 // barriers between dependent passes.  Used once a level is small enough
-// (<= 512 cells) that CTA-wide barriers would cost more than the work.
+// (A.tail_cells, tuned) that team-wide barriers would cost more than the work.
 template <int P>
 __device__ void warp_tail_vcycle(const KArena& A, const KDesc& D, int l0, int nu, int coarse_sweeps, float omega) {
     const int t = threadIdx.x & 31, T = 32;
@@ -612,8 +612,6 @@ __device__ void warp_tail_vcycle(const KArena& A, const KDesc& D, int l0, int nu
             for (int c = 7; c >= 0; c--) { op_smoothc<P>(A, D, l, t, T, c); __syncwarp(); }
     }
 }
-
-constexpr int kWarpTailCells = 512;
 
 }  // namespace
 }  // namespace kappa

@@ -37,7 +37,7 @@ bool valid(const pfsf_tuning& t) {
     const bool launch = (t.cluster == 1 || t.cluster == 4 || t.cluster == 8) && t.cluster_min_voxels >= 0 &&
                         t.grid_min_voxels >= 0 && t.warp_max_voxels >= 0 && t.cheb_k >= 1 && t.cheb_k <= 4;
     const bool solver = !has_solver(t) || (t.cheb_lower > 0.0f && t.cheb_lower < 1.0f && t.coarse_weight > 0.0f &&
-                                           t.coarse_weight < 2.0f);
+                                           t.coarse_weight < 2.0f && t.tail_cells >= 0 && t.tail_cells <= (1 << 20));
     return launch && solver;
 }
 
@@ -90,6 +90,7 @@ void Engine::load_tuning() {
         else if (k == "cheb_k") t.cheb_k = (int32_t)v;
         else if (k == "cheb_lower") t.cheb_lower = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
         else if (k == "coarse_weight") t.coarse_weight = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
+        else if (k == "tail_cells") t.tail_cells = (int32_t)v;
     }
     if (found && valid(t)) {
         set_tuning(&t);
@@ -106,6 +107,7 @@ void Engine::load_tuning() {
     if (const char* f = std::getenv("PFSF_CHEB_K")) { cheb_k_ = std::atoi(f); over = true; }
     if (const char* f = std::getenv("PFSF_CHEB_LOWER")) { cheb_lower_ = std::strtof(f, nullptr); over = true; }
     if (const char* f = std::getenv("PFSF_COARSE_WEIGHT")) { coarse_weight_ = std::strtof(f, nullptr); over = true; }
+    if (const char* f = std::getenv("PFSF_TAIL_CELLS")) { tail_cells_ = std::atoi(f); over = true; }
     if (over) tuning_source_ = PFSF_TUNING_ENV;
 }
 
@@ -121,6 +123,7 @@ pfsf_result Engine::get_tuning(pfsf_tuning* out) const {
     t.source = tuning_source_;
     t.cheb_lower = cheb_lower_;
     t.coarse_weight = coarse_weight_;
+    t.tail_cells = tail_cells_;
     // a caller's older, shorter struct gets the fields it has
     const size_t n = out->struct_bytes > 0 ? std::min(sizeof(t), (size_t)out->struct_bytes) : sizeof(t);
     std::memcpy(out, &t, n);
@@ -137,6 +140,7 @@ pfsf_result Engine::set_tuning(const pfsf_tuning* in) {
     if (has_solver(*in)) {
         cheb_lower_ = in->cheb_lower;
         coarse_weight_ = in->coarse_weight;
+        tail_cells_ = in->tail_cells;
     }
     tuning_source_ = PFSF_TUNING_CALLER;
     return PFSF_OK;

@@ -113,13 +113,15 @@ class Tuning(C.Structure):
     SOURCES = {0: "default", 1: "file", 2: "env", 3: "caller"}
     _fields_ = [("struct_bytes", C.c_int32), ("cluster", C.c_int32), ("cluster_min_voxels", C.c_int64),
                 ("grid_min_voxels", C.c_int64), ("warp_max_voxels", C.c_int64), ("cheb_k", C.c_int32),
-                ("source", C.c_int32), ("cheb_lower", C.c_float), ("coarse_weight", C.c_float)]
+                ("source", C.c_int32), ("cheb_lower", C.c_float), ("coarse_weight", C.c_float),
+                ("tail_cells", C.c_int32), ("reserved", C.c_int32)]
 
     def as_dict(self):
         return {"cluster": self.cluster, "cluster_min_voxels": self.cluster_min_voxels,
                 "grid_min_voxels": self.grid_min_voxels, "warp_max_voxels": self.warp_max_voxels,
                 "cheb_k": self.cheb_k, "cheb_lower": round(float(self.cheb_lower), 6),
                 "coarse_weight": round(float(self.coarse_weight), 6),
+                "tail_cells": self.tail_cells,
                 "source": self.SOURCES.get(self.source, str(self.source))}
 
 

@@ -11,7 +11,7 @@ from pfsf_b200 import autotune, capi
 pytestmark = pytest.mark.gpu
 
 ENV = ("PFSF_CLUSTER", "PFSF_CLUSTER_MIN_VOXELS", "PFSF_GRID_MIN_VOXELS", "PFSF_WARP_MAX_VOXELS", "PFSF_CHEB_K",
-       "PFSF_CHEB_LOWER", "PFSF_COARSE_WEIGHT")
+       "PFSF_CHEB_LOWER", "PFSF_COARSE_WEIGHT", "PFSF_TAIL_CELLS")
 
 
 def _same(t, best):
@@ -27,7 +27,8 @@ def test_autotune_cache_is_read_at_init(lib_built, tmp_path, monkeypatch):
     eng = capi.Engine(cfg)
     assert eng.init() == capi.PFSF_OK, "CUDA device required"
     best, trials = autotune.tune(eng, islands=48, target_active=3e5, big_dims=None, reps=1, budget_s=60.0,
-                                 candidates={"cluster": [1, 4], "cheb_k": [2, 3], "coarse_weight": [1.4, 1.8]})
+                                 candidates={"cluster": [1, 4], "cheb_k": [2, 3], "coarse_weight": [1.4, 1.8],
+                                             "tail_cells": [64, 512]})
     assert len(trials) >= 2 and np.isfinite(trials[0]["ms"])
     # the tuner leaves the winner set on its engine
     rc, t = eng.tuning()
@@ -48,6 +49,7 @@ def test_autotune_cache_is_read_at_init(lib_built, tmp_path, monkeypatch):
     assert e2.set_tuning(cheb_k=0) == capi.PFSF_ERROR_INVALID_ARG
     assert e2.set_tuning(coarse_weight=2.0) == capi.PFSF_ERROR_INVALID_ARG
     assert e2.set_tuning(cheb_lower=0.0) == capi.PFSF_ERROR_INVALID_ARG
+    assert e2.set_tuning(tail_cells=-1) == capi.PFSF_ERROR_INVALID_ARG
     rc, t3 = e2.tuning()
     assert t3.cluster == best["cluster"] and t3.cheb_k == best["cheb_k"]
     # an environment override wins over the file

@@ -170,3 +170,39 @@ def test_wcycle_converges_and_matches_oracle(lib_built):
         iters[cyc] = st.inner_iterations_total
     assert iters[capi.MG_W] <= iters[capi.MG_V], iters
     e.close()
+
+
+def test_tail_threshold_changes_no_result(lib_built):
+    """The coarse-level size from which one warp runs the rest of the V-cycle
+    (tail_cells, a tuned launch shape) moves work between the team and its
+    leader warp without changing any arithmetic: every threshold gives the
+    same iterations and the same solution, bit for bit, on islands solved by
+    CTAs and by a cluster."""
+    e = capi.Engine(capi.default_config(max_island_size=1 << 26, tick_budget_ms=1 << 30))
+    assert e.init() == capi.PFSF_OK
+    isls = [synth.noise_island((40, 36, 28), seed=81), synth.noise_island((72, 64, 40), seed=82),
+            synth.solid_block((20, 18, 16), seed=83)]
+    keep = []
+    for k, isl in enumerate(isls):
+        phi = np.zeros(isl.n, np.float32)
+        keep.append(phi)
+        assert e.add_island(k + 1, isl.dims) == capi.PFSF_OK
+        assert e.register_kappa(k + 1, phi, isl.source, isl.kappa, isl.vtype) == capi.PFSF_OK
+    ids = [1, 2, 3]
+    e.set_solve_mode(capi.SOLVE_BATCHED)
+    e.set_precision(capi.PREC_BF16)
+    assert e.set_tuning(cluster=4, cluster_min_voxels=150000) == capi.PFSF_OK  # island 2 on a cluster
+    ref = None
+    for tail in (512, 0, 64, 4096):
+        assert e.set_tuning(tail_cells=tail) == capi.PFSF_OK
+        rc, st = e.solve(ids, tol=1e-6, flags=capi.SOLVE_COLD_START)
+        assert rc == capi.PFSF_OK and st.islands_converged == 3
+        xs = [e.read_solution64(i, isls[i - 1].n)[1].copy() for i in ids]
+        got = (st.inner_iterations_total, xs)
+        if ref is None:
+            ref = got
+            continue
+        assert got[0] == ref[0], (tail, got[0], ref[0])
+        for a, b in zip(got[1], ref[1]):
+            assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), tail
+    e.close()
