@@ -183,6 +183,8 @@ typedef struct pfsf_tuning {
     int32_t reserved;
 } pfsf_tuning;
 
+/* out->struct_bytes: the caller's sizeof(pfsf_tuning) (an older, shorter struct gets the fields
+ * it has; 0 or less: the whole current struct is written). */
 PFSF_API pfsf_result pfsf_get_tuning(pfsf_engine engine, pfsf_tuning* out);
 /* INVALID_ARG for out-of-range values (nothing changes then). */
 PFSF_API pfsf_result pfsf_set_tuning(pfsf_engine engine, const pfsf_tuning* in);
