@@ -59,6 +59,7 @@ struct KDesc {
     unsigned long long t_start, t_end;  // %globaltimer (ns) around the island's solve
     unsigned long long t_setup, t_precond;  // ns in the hierarchy build / in V-cycles (batched mode)
     unsigned long long t_vfine, t_vcoarse, t_vtail;  // V-cycle split: fine level, team coarse levels, tail
+    unsigned long long t_mark, t_pmark;  // the team leader's last lap marks (timing scratch)
     int team, team_ctas;  // pfsf_island_team of the solving team and its CTAs (batched mode)
 };
 

@@ -389,20 +389,33 @@ __device__ void warp_tail_cheb(const KArena& A, const KDesc& D, int l0) {
 
 // V-cycle with Chebyshev smoothing on every level (same structure as
 // team_vcycle).  Time spent in each part (the leader's clock, between
-// barriers) accumulates into vt.
-struct VTimes {
-    unsigned long long fine = 0, coarse = 0, tail = 0;
-};
+// barriers) accumulates in the island's descriptor: the leader keeps its lap
+// marks there, in global memory, so that no thread of the team carries
+// timestamps in registers through the passes.
+template <class TeamT>
+__device__ __forceinline__ void tmark(const TeamT& tm, const KDesc& D, unsigned long long KDesc::*mark) {
+    if (tm.leader()) const_cast<KDesc&>(D).*mark = globaltimer();
+}
+template <class TeamT>
+__device__ __forceinline__ void tlap(const TeamT& tm, const KDesc& D, unsigned long long KDesc::*mark,
+                                     unsigned long long KDesc::*acc) {
+    if (tm.leader()) {
+        KDesc& d = const_cast<KDesc&>(D);
+        const unsigned long long now = globaltimer();
+        d.*acc += now - d.*mark;
+        d.*mark = now;
+    }
+}
 
 template <int P, class TeamT>
-__device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTimes& vt) {
+__device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm) {
     const int t = (int)tm.t(), T = (int)tm.T();
     const int L = D.nlev;
-    unsigned long long c0 = globaltimer();
+    tmark(tm, D, &KDesc::t_mark);
     if (L <= 1) {
         team_cheb0<P>(A, D, tm, true);
         team_cheb0<P>(A, D, tm, false);
-        vt.fine += globaltimer() - c0;
+        tlap(tm, D, &KDesc::t_mark, &KDesc::t_vfine);
         return;
     }
     int l0 = 1;
@@ -410,15 +423,13 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
     team_cheb0<P>(A, D, tm, true);
     t_restrict0<P>(A, D, tm);
     tm.sync();
-    unsigned long long c1 = globaltimer();
-    vt.fine += c1 - c0;
+    tlap(tm, D, &KDesc::t_mark, &KDesc::t_vfine);
     for (int l = 1; l < l0; l++) {
         team_chebc<P>(A, D, l, tm, true);
         op_restrictc<P>(A, D, l, t, T);
         tm.sync();
     }
-    c0 = globaltimer();
-    vt.coarse += c0 - c1;
+    tlap(tm, D, &KDesc::t_mark, &KDesc::t_vcoarse);
     if (D.lev[l0].n <= A.tail_cells) {
         if (tm.leader_warp()) warp_tail_cheb<P>(A, D, l0);
         tm.sync();
@@ -426,8 +437,7 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
         team_chebc<P>(A, D, L - 1, tm, true);
         for (int s = 1; s < A.coarse_sweeps; s++) team_chebc<P>(A, D, L - 1, tm, false);
     }
-    c1 = globaltimer();
-    vt.tail += c1 - c0;
+    tlap(tm, D, &KDesc::t_mark, &KDesc::t_vtail);
     // prolongate into whichever array makes the post-smoothing end in x / z
     const bool odd = (A.cheb_k & 1) != 0;
     for (int l = l0 - 1; l >= 1; l--) {
@@ -463,24 +473,26 @@ __device__ void team_vcycle_cheb(const KArena& A, const KDesc& D, TeamT& tm, VTi
             team_chebc<P>(A, D, l, tm, false, odd);
         }
     }
-    c0 = globaltimer();
-    vt.coarse += c0 - c1;
+    tlap(tm, D, &KDesc::t_mark, &KDesc::t_vcoarse);
     op_prolong0_to(A, D, t, T, A.omega_c, A.z + D.off, odd ? A.q + D.off : A.z + D.off);
     tm.sync();
     team_cheb0<P>(A, D, tm, false, odd);
-    vt.fine += globaltimer() - c0;
+    tlap(tm, D, &KDesc::t_mark, &KDesc::t_vfine);
 }
 
 template <int P, class TeamT>
-__device__ __forceinline__ void precondition(const KArena& A, const KDesc& D, TeamT& tm, VTimes& vt) {
-    if (A.smoother == 1) team_vcycle_cheb<P>(A, D, tm, vt);
+__device__ __forceinline__ void precondition(const KArena& A, const KDesc& D, TeamT& tm) {
+    if (A.smoother == 1) team_vcycle_cheb<P>(A, D, tm);
     else team_vcycle<P>(A, D, tm);
 }
 
 template <int P, class R, class TeamT>
 __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
     const int t = (int)tm.t(), T = (int)tm.T();
-    const unsigned long long t0 = globaltimer();
+    if (tm.leader()) {
+        D.t_start = globaltimer();
+        D.t_precond = D.t_vfine = D.t_vcoarse = D.t_vtail = 0;
+    }
     if (D.nlev > 1) {
         op_build1<P>(A, D, t, T);
         tm.sync();
@@ -498,13 +510,12 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         vop_zero(t, T, (int)D.n, A.q + D.off);
         flat_lists(A, D, *tm.fs, tm);
     }
-    const unsigned long long t_built = globaltimer();
-    unsigned long long t_pc = 0;  // time in V-cycles (the leader's clock, between barriers)
-    VTimes vt;
+    if (tm.leader()) D.t_setup = globaltimer() - D.t_start;
+    // time in V-cycles (the leader's clock, between barriers)
     auto timed_precondition = [&]() {
-        const unsigned long long a = globaltimer();
-        precondition<P>(A, D, tm, vt);
-        t_pc += globaltimer() - a;
+        tmark(tm, D, &KDesc::t_pmark);
+        precondition<P>(A, D, tm);
+        tlap(tm, D, &KDesc::t_pmark, &KDesc::t_precond);
     };
     double relres = 1.0, bn = 0.0;
     int inner_total = 0, outer = 0;
@@ -555,13 +566,7 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         D.inner_iters = inner_total;
         D.outer_iters = outer;
         D.converged = conv ? 1 : 0;
-        D.t_start = t0;
         D.t_end = globaltimer();
-        D.t_setup = t_built - t0;
-        D.t_precond = t_pc;
-        D.t_vfine = vt.fine;
-        D.t_vcoarse = vt.coarse;
-        D.t_vtail = vt.tail;
         D.team = TeamT::kKind;
         D.team_ctas = tm.ctas();
     }
