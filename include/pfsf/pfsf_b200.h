@@ -160,7 +160,8 @@ PFSF_API pfsf_result pfsf_island_solve_report(pfsf_engine engine, int32_t island
  * PFSF_TUNE_FILE, else tune/pfsf_tune.txt beside the library's lib/
  * directory -- then from the PFSF_CLUSTER, PFSF_CLUSTER_MIN_VOXELS,
  * PFSF_GRID_MIN_VOXELS, PFSF_WARP_MAX_VOXELS, PFSF_CHEB_K, PFSF_CHEB_LOWER,
- * PFSF_COARSE_WEIGHT, PFSF_TAIL_CELLS variables when set; built-in defaults otherwise. */
+ * PFSF_COARSE_WEIGHT, PFSF_TAIL_CELLS, PFSF_COARSE_SWEEPS, PFSF_INNER_ETA variables when
+ * set; built-in defaults otherwise. */
 typedef enum pfsf_tuning_source {
     PFSF_TUNING_DEFAULT = 0,  /* built-in defaults */
     PFSF_TUNING_FILE = 1,     /* the tuning file's section for this GPU */
@@ -180,6 +181,9 @@ typedef struct pfsf_tuning {
     float cheb_lower;             /* Chebyshev interval [cheb_lower * lmax, lmax], 0 < cheb_lower < 1 */
     float coarse_weight;          /* coarse-correction weight of the V-cycle, 0 < w < 2 (keeps it SPD) */
     int32_t tail_cells;           /* coarse levels of at most this many cells run on one warp, 0..1048576 */
+    int32_t coarse_sweeps;        /* smoothing steps on the coarsest level, 1..16 */
+    float inner_eta;              /* inner PCG stops at max(inner_eta, 0.3 tol / relres) of the outer residual,
+                                     1e-6 < inner_eta < 1 */
     int32_t reserved;
 } pfsf_tuning;
 

@@ -265,6 +265,8 @@ private:
     float cheb_lower_ = 0.1f;             // PFSF_CHEB_LOWER: Chebyshev interval [lower * lmax, lmax]
     float coarse_weight_ = 1.8f;          // PFSF_COARSE_WEIGHT: V-cycle coarse-correction weight
     int tail_cells_ = 512;                // PFSF_TAIL_CELLS: coarse levels this small run on one warp
+    int coarse_sweeps_ = 4;               // PFSF_COARSE_SWEEPS: smoothing steps on the coarsest level
+    float inner_eta_ = 1e-4f;             // PFSF_INNER_ETA: floor of the inner PCG's relative stop
     int tuning_source_ = PFSF_TUNING_DEFAULT;
     int mg_cycle_ = 0;                    // 0 V-cycle, 1 W-cycle (batched tolerance solve)
     void load_tuning();                   // tuning file, then environment overrides (init)

@@ -271,12 +271,12 @@ bool Engine::collect_kappa_set(const int32_t* ids, int32_t count, std::vector<Is
 KArena Engine::solve_params(double tol, int32_t max_iter) const {
     KArena k = arena_->dev;
     k.tol = tol;
-    k.eta_min = 1e-4;
+    k.eta_min = (double)inner_eta_;
     k.max_outer = 8;
     k.max_inner = max_iter > 0 ? max_iter : 500;
     k.omega_c = coarse_weight_;
     k.nu = 2;
-    k.coarse_sweeps = 4;
+    k.coarse_sweeps = coarse_sweeps_;
     const bool batched = solve_mode_ == PFSF_SOLVE_BATCHED;
     k.fp64_dots = batched ? 1 : 0;
     // batched: Chebyshev smoothing (one stencil pass per step, few barriers);

@@ -37,7 +37,9 @@ bool valid(const pfsf_tuning& t) {
     const bool launch = (t.cluster == 1 || t.cluster == 4 || t.cluster == 8) && t.cluster_min_voxels >= 0 &&
                         t.grid_min_voxels >= 0 && t.warp_max_voxels >= 0 && t.cheb_k >= 1 && t.cheb_k <= 4;
     const bool solver = !has_solver(t) || (t.cheb_lower > 0.0f && t.cheb_lower < 1.0f && t.coarse_weight > 0.0f &&
-                                           t.coarse_weight < 2.0f && t.tail_cells >= 0 && t.tail_cells <= (1 << 20));
+                                           t.coarse_weight < 2.0f && t.tail_cells >= 0 && t.tail_cells <= (1 << 20) &&
+                                           t.coarse_sweeps >= 1 && t.coarse_sweeps <= 16 && t.inner_eta > 1e-6f &&
+                                           t.inner_eta < 1.0f);
     return launch && solver;
 }
 
@@ -91,6 +93,8 @@ void Engine::load_tuning() {
         else if (k == "cheb_lower") t.cheb_lower = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
         else if (k == "coarse_weight") t.coarse_weight = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
         else if (k == "tail_cells") t.tail_cells = (int32_t)v;
+        else if (k == "coarse_sweeps") t.coarse_sweeps = (int32_t)v;
+        else if (k == "inner_eta") t.inner_eta = std::strtof(trim(line.substr(eq + 1)).c_str(), nullptr);
     }
     if (found && valid(t)) {
         set_tuning(&t);
@@ -108,6 +112,8 @@ void Engine::load_tuning() {
     if (const char* f = std::getenv("PFSF_CHEB_LOWER")) { cheb_lower_ = std::strtof(f, nullptr); over = true; }
     if (const char* f = std::getenv("PFSF_COARSE_WEIGHT")) { coarse_weight_ = std::strtof(f, nullptr); over = true; }
     if (const char* f = std::getenv("PFSF_TAIL_CELLS")) { tail_cells_ = std::atoi(f); over = true; }
+    if (const char* f = std::getenv("PFSF_COARSE_SWEEPS")) { coarse_sweeps_ = std::atoi(f); over = true; }
+    if (const char* f = std::getenv("PFSF_INNER_ETA")) { inner_eta_ = std::strtof(f, nullptr); over = true; }
     if (over) tuning_source_ = PFSF_TUNING_ENV;
 }
 
@@ -124,6 +130,8 @@ pfsf_result Engine::get_tuning(pfsf_tuning* out) const {
     t.cheb_lower = cheb_lower_;
     t.coarse_weight = coarse_weight_;
     t.tail_cells = tail_cells_;
+    t.coarse_sweeps = coarse_sweeps_;
+    t.inner_eta = inner_eta_;
     // a caller's older, shorter struct gets the fields it has
     const size_t n = out->struct_bytes > 0 ? std::min(sizeof(t), (size_t)out->struct_bytes) : sizeof(t);
     std::memcpy(out, &t, n);
@@ -141,6 +149,8 @@ pfsf_result Engine::set_tuning(const pfsf_tuning* in) {
         cheb_lower_ = in->cheb_lower;
         coarse_weight_ = in->coarse_weight;
         tail_cells_ = in->tail_cells;
+        coarse_sweeps_ = in->coarse_sweeps;
+        inner_eta_ = in->inner_eta;
     }
     tuning_source_ = PFSF_TUNING_CALLER;
     return PFSF_OK;

@@ -7,7 +7,8 @@ for big islands (1, 4, 8 CTAs), the island size from which clusters take
 over from single CTAs, the size below which single warps take islands, the
 Chebyshev smoothing degree and the lower end of its interval, the V-cycle's
 coarse-correction weight, the coarse-level size from which one warp runs the
-rest of the cycle, and the size from which one island takes the whole GPU.  Method: timed trials -- the device time of a resident solve to
+rest of the cycle, the smoothing steps on the coarsest level, the inner
+PCG's stopping floor, and the size from which one island takes the whole GPU.  Method: timed trials -- the device time of a resident solve to
 the benchmark tolerance (median of `reps`) -- by coordinate descent from the
 current values, on a size-bucketed island set drawn like the benchmark's
 (per-axis log-uniform sides scaled to the set's active-voxel target); the
@@ -29,8 +30,8 @@ from . import capi, synth
 
 DEFAULT_FILE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tune", "pfsf_tune.txt")
 KEYS = ("cluster", "cluster_min_voxels", "grid_min_voxels", "warp_max_voxels", "cheb_k", "cheb_lower",
-        "coarse_weight", "tail_cells")
-FLOAT_KEYS = ("cheb_lower", "coarse_weight")
+        "coarse_weight", "tail_cells", "coarse_sweeps", "inner_eta")
+FLOAT_KEYS = ("cheb_lower", "coarse_weight", "inner_eta")
 CANDIDATES = {
     "cluster": [1, 4, 8],
     "cluster_min_voxels": [32768, 65536, 131072, 262144, 524288],
@@ -42,6 +43,8 @@ CANDIDATES = {
     # the benchmark set, not enough to trade robustness on other islands
     "coarse_weight": [1.0, 1.4, 1.6, 1.8],
     "tail_cells": [0, 64, 128, 256, 512, 2048],
+    "coarse_sweeps": [1, 2, 3, 4, 6],
+    "inner_eta": [3e-5, 1e-4, 3e-4, 1e-3],
 }
 
 
@@ -105,7 +108,7 @@ def tune(eng, islands=4096, target_active=6.0e7, big_dims=(160, 160, 96), tol=1e
 
     best_ms = trial(best)
     for key in ("cluster", "cluster_min_voxels", "tail_cells", "cheb_k", "cheb_lower", "coarse_weight",
-                "warp_max_voxels"):
+                "coarse_sweeps", "inner_eta", "warp_max_voxels"):
         for v in cands.get(key, []):
             if time.monotonic() > t_end:
                 break

@@ -114,7 +114,8 @@ class Tuning(C.Structure):
     _fields_ = [("struct_bytes", C.c_int32), ("cluster", C.c_int32), ("cluster_min_voxels", C.c_int64),
                 ("grid_min_voxels", C.c_int64), ("warp_max_voxels", C.c_int64), ("cheb_k", C.c_int32),
                 ("source", C.c_int32), ("cheb_lower", C.c_float), ("coarse_weight", C.c_float),
-                ("tail_cells", C.c_int32), ("reserved", C.c_int32)]
+                ("tail_cells", C.c_int32), ("coarse_sweeps", C.c_int32), ("inner_eta", C.c_float),
+                ("reserved", C.c_int32)]
 
     def as_dict(self):
         return {"cluster": self.cluster, "cluster_min_voxels": self.cluster_min_voxels,
@@ -122,6 +123,7 @@ class Tuning(C.Structure):
                 "cheb_k": self.cheb_k, "cheb_lower": round(float(self.cheb_lower), 6),
                 "coarse_weight": round(float(self.coarse_weight), 6),
                 "tail_cells": self.tail_cells,
+                "coarse_sweeps": self.coarse_sweeps, "inner_eta": round(float(self.inner_eta), 8),
                 "source": self.SOURCES.get(self.source, str(self.source))}
 
 
@@ -329,7 +331,7 @@ class Engine:
         """pfsf_set_tuning with the current values updated by kw."""
         rc, t = self.tuning()
         for k, v in kw.items():
-            setattr(t, k, float(v) if k in ("cheb_lower", "coarse_weight") else int(v))
+            setattr(t, k, float(v) if k in ("cheb_lower", "coarse_weight", "inner_eta") else int(v))
         t.struct_bytes = C.sizeof(Tuning)
         return self.L.pfsf_set_tuning(self.h, C.byref(t))
 

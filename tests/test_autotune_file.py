@@ -3,7 +3,7 @@ place, read back by the same rules the engine uses (no GPU needed)."""
 from pfsf_b200 import autotune
 
 P = {"cluster": 4, "cluster_min_voxels": 262144, "grid_min_voxels": 2097152, "warp_max_voxels": 0, "cheb_k": 3,
-     "cheb_lower": 0.15, "coarse_weight": 1.6, "tail_cells": 128}
+     "cheb_lower": 0.15, "coarse_weight": 1.6, "tail_cells": 128, "coarse_sweeps": 3, "inner_eta": 0.0003}
 
 
 def _read(path):

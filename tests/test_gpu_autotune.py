@@ -11,7 +11,7 @@ from pfsf_b200 import autotune, capi
 pytestmark = pytest.mark.gpu
 
 ENV = ("PFSF_CLUSTER", "PFSF_CLUSTER_MIN_VOXELS", "PFSF_GRID_MIN_VOXELS", "PFSF_WARP_MAX_VOXELS", "PFSF_CHEB_K",
-       "PFSF_CHEB_LOWER", "PFSF_COARSE_WEIGHT", "PFSF_TAIL_CELLS")
+       "PFSF_CHEB_LOWER", "PFSF_COARSE_WEIGHT", "PFSF_TAIL_CELLS", "PFSF_COARSE_SWEEPS", "PFSF_INNER_ETA")
 
 
 def _same(t, best):
@@ -50,6 +50,8 @@ def test_autotune_cache_is_read_at_init(lib_built, tmp_path, monkeypatch):
     assert e2.set_tuning(coarse_weight=2.0) == capi.PFSF_ERROR_INVALID_ARG
     assert e2.set_tuning(cheb_lower=0.0) == capi.PFSF_ERROR_INVALID_ARG
     assert e2.set_tuning(tail_cells=-1) == capi.PFSF_ERROR_INVALID_ARG
+    assert e2.set_tuning(coarse_sweeps=0) == capi.PFSF_ERROR_INVALID_ARG
+    assert e2.set_tuning(inner_eta=1.0) == capi.PFSF_ERROR_INVALID_ARG
     rc, t3 = e2.tuning()
     assert t3.cluster == best["cluster"] and t3.cheb_k == best["cheb_k"]
     # an environment override wins over the file
