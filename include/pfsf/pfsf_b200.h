@@ -53,9 +53,10 @@ typedef struct pfsf_solve_stats {
     int32_t islands_converged;
     int32_t max_iterations;  /* largest outer iteration count over islands */
     double max_rel_residual; /* largest final ||s - A phi|| / ||s|| (FP64) */
-    float device_ms;         /* solve time on the engine stream (CUDA events) */
-    float upload_ms;
-    float readback_ms;
+    float device_ms;         /* solve time on the engine stream (CUDA events); in batched mode it
+                                includes the teams' reads of mapped inputs and writes of phi */
+    float upload_ms;         /* input copies and preparation before the solve */
+    float readback_ms;       /* phi conversion and copies after the solve */
     int32_t kernel_launches; /* kernels launched by the solve */
     int64_t inner_iterations_total; /* sum over islands of inner PCG iterations */
     double algorithmic_bytes;       /* compulsory bytes of every pass the solve made:

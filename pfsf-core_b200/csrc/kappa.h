@@ -5,6 +5,8 @@
 
 #include <vector>
 
+#include "arena_io.h"
+
 namespace pfsf_b200 {
 
 // Levels of the hierarchy (fine + 4 coarse).  Measured with 8 (coarsest
@@ -104,6 +106,12 @@ struct KArena {
     // offsets per (tile, plane) at desc.soff (built by each solve)
     uint32_t* flist;
     int* fstart;
+    // the caller's host arrays, device-mapped, per island (arena_io.h).
+    // ingest: each team reads its island's inputs from there before the
+    // solve (prepared as k_prepare does; x64 = 0 with cold); emit: each team
+    // writes its FP32 solution into e and the caller's phi array after it.
+    const kappa::IslandIO* io;
+    int ingest, cold, emit;
 };
 
 struct KappaState {

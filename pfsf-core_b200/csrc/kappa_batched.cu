@@ -486,12 +486,58 @@ __device__ __forceinline__ void precondition(const KArena& A, const KDesc& D, Te
     else team_vcycle<P>(A, D, tm);
 }
 
+// The island's inputs straight from the caller's mapped host arrays into
+// the arena, prepared as k_prepare prepares them (kappa_plain.cu): kappa
+// clamped at 0 and 0 on air, its preconditioner rounding, the source 0 off
+// solid voxels, x64 = phi0 on solid voxels (0 elsewhere, 0 everywhere with
+// a cold start).  Each team reads its own island while the other teams
+// solve theirs, so the host-link transfer overlaps the solve.
+__device__ __forceinline__ void team_ingest(const KArena& A, const KDesc& D, const kappa::IslandIO& io, int t,
+                                            int T) {
+    uint8_t* type = const_cast<uint8_t*>(A.type) + D.off;
+    float* k32 = const_cast<float*>(A.k32) + D.off;
+    uint16_t* k16 = const_cast<uint16_t*>(A.k16) + D.off;
+    float* b = const_cast<float*>(A.b) + D.off;
+    double* x64 = A.x64 + D.off;
+    const int64_t n = D.n;
+#pragma unroll 4
+    for (int64_t i = t; i < n; i += T) {
+        const uint8_t ty = io.h_type[i];
+        const float kin = io.h_kappa[i], src = io.h_source[i], phi0 = io.h_phi[i];
+        const float k = ty == kAir ? 0.0f : fmaxf(kin, 0.0f);
+        type[i] = ty;
+        k32[i] = k;
+        if (A.prec == 1) k16[i] = __bfloat16_as_ushort(__float2bfloat16_rn(k));
+        else if (A.prec == 2) k16[i] = __half_as_ushort(__float2half_rn(k));
+        b[i] = ty == kSolid ? src : 0.0f;
+        x64[i] = (ty == kSolid && !A.cold) ? (double)phi0 : 0.0;
+    }
+}
+
+// The island's FP32 solution into the arena's e and, for a mapped island,
+// into the caller's phi array (posted writes over the host link).
+__device__ __forceinline__ void team_emit(const KArena& A, const KDesc& D, const kappa::IslandIO& io, int t, int T) {
+    const double* x64 = A.x64 + D.off;
+    float* e = A.e + D.off;
+    const int64_t n = D.n;
+    for (int64_t i = t; i < n; i += T) {
+        const float v = (float)x64[i];
+        e[i] = v;
+        if (io.h_phi_out) io.h_phi_out[i] = v;
+    }
+}
+
 template <int P, class R, class TeamT>
 __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
     const int t = (int)tm.t(), T = (int)tm.T();
     if (tm.leader()) {
         D.t_start = globaltimer();
         D.t_precond = D.t_vfine = D.t_vcoarse = D.t_vtail = 0;
+    }
+    const kappa::IslandIO* io = (A.ingest || A.emit) ? &A.io[&D - A.desc] : nullptr;
+    if (A.ingest && io->h_type) {
+        team_ingest(A, D, *io, t, T);
+        tm.sync();
     }
     if (D.nlev > 1) {
         op_build1<P>(A, D, t, T);
@@ -560,6 +606,7 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
         t_accumulate(A, D, tm);
         tm.sync();
     }
+    if (A.emit) team_emit(A, D, *io, t, T);
     if (tm.leader()) {
         D.relres = relres;
         D.bnorm = bn;

@@ -285,6 +285,8 @@ KArena Engine::solve_params(double tol, int32_t max_iter) const {
     k.wcycle = (batched && mg_cycle_ == 1) ? 1 : 0;
     k.cheb_k = std::max(1, std::min(4, cheb_k_));
     k.tail_cells = tail_cells_;
+    k.io = arena_->d_io;
+    k.ingest = k.cold = k.emit = 0;
     {
         const double lmax = 2.0, lmin = lmax * (double)cheb_lower_;
         const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
@@ -345,7 +347,8 @@ pfsf_result Engine::run_solve(const KArena& k, int64_t& nl) {
                                      (double)k.nu, (double)k.coarse_sweeps, (double)k.fp64_dots, (double)k.smoother,
                                      (double)k.cheb_k, (double)k.wcycle, (double)k.prec, (double)nbig, (double)nsmall,
                                      (double)cluster_size_, (double)num_sms_, (double)nisl, (double)k.cheb_c2[0],
-                                     (double)k.cheb_c1[1], (double)k.tail_cells};
+                                     (double)k.cheb_c1[1], (double)k.tail_cells, (double)k.ingest, (double)k.cold,
+                                     (double)k.emit};
     *flag = 0;
     if (ngiant == 0 && A.launched && !A.graph_off) {
         if (A.solve_exec && A.solve_key != key) {
@@ -454,14 +457,18 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     }
     Arena& A = *arena_;
     if (A.b_stale) do_upload = true;  // an adjoint solve replaced the sources
-    const KArena k = solve_params(tol, max_iter);
+    KArena k = solve_params(tol, max_iter);
+    // batched: every team reads its mapped island's inputs before its solve and
+    // writes its solution back after it, inside the persistent launch, so the
+    // host-link traffic overlaps the other teams' solves
+    const bool fuse = solve_mode_ == PFSF_SOLVE_BATCHED && A.io_any;
 
     cudaEvent_t ev[4];
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], stream_);
     if (do_upload) {
-        // mapped islands in one gather launch, the others by copies
-        if (A.io_any) {
+        // mapped islands in one gather launch (or by their teams), the others by copies
+        if (A.io_any && !fuse) {
             kappa::launch_arena_upload(stream_, A.d_io, (int)set.size(), A.io_blocks, const_cast<uint8_t*>(k.type),
                                        const_cast<float*>(k.k32), const_cast<float*>(k.b), k.e);
             launches_++;
@@ -487,15 +494,22 @@ pfsf_result Engine::solve_to_tolerance(const int32_t* ids, int32_t count, double
     }
     cudaEventRecord(ev[1], stream_);
     if (flags & PFSF_SOLVE_COLD_START) cudaMemsetAsync(k.x64, 0, (size_t)A.nfine * 8, stream_);
+    const bool readback = !(flags & PFSF_SOLVE_NO_READBACK);
+    k.ingest = (fuse && do_upload) ? 1 : 0;
+    k.cold = (flags & PFSF_SOLVE_COLD_START) ? 1 : 0;
+    k.emit = (fuse && readback) ? 1 : 0;
     std::vector<KDesc> res;
     int64_t nl = 0;
     if (pfsf_result rc = run_solve(k, nl); rc != PFSF_OK) return rc;
     cudaEventRecord(ev[2], stream_);
-    if (!(flags & PFSF_SOLVE_NO_READBACK)) {
-        // e = (float)x64 for every island, written to mapped callers' phi in the same launch
-        kappa::launch_arena_readback(stream_, A.d_io, (int)set.size(), A.io_blocks, k.x64, k.e);
-        launches_++;
-        nl++;
+    if (readback) {
+        // e = (float)x64 for every island (by the teams when fused), written to
+        // mapped callers' phi in the same launch; the others copied from e
+        if (!fuse) {
+            kappa::launch_arena_readback(stream_, A.d_io, (int)set.size(), A.io_blocks, k.x64, k.e);
+            launches_++;
+            nl++;
+        }
         for (size_t q = 0; q < set.size(); q++) {
             if (A.io[q].h_phi_out) continue;
             const Island* s = set[q];

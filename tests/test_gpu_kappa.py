@@ -206,3 +206,49 @@ def test_tail_threshold_changes_no_result(lib_built):
         for a, b in zip(got[1], ref[1]):
             assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), tail
     e.close()
+
+
+def test_mapped_and_copied_islands_in_one_solve(lib_built):
+    """One batched solve over an island whose arrays the engine maps into the
+    device address space (the teams read its inputs and write its phi inside
+    the persistent launch) and one whose arrays were page-locked by another
+    allocator (torch pinned memory: the engine cannot map them and copies
+    them instead).  Both islands converge and each caller phi array holds
+    the FP32 rounding of the island's FP64 solution, bit for bit."""
+    torch = pytest.importorskip("torch")
+    e = capi.Engine(capi.default_config(max_island_size=1 << 26, tick_budget_ms=1 << 30))
+    assert e.init() == capi.PFSF_OK
+    e.set_solve_mode(capi.SOLVE_BATCHED)
+    e.set_precision(capi.PREC_BF16)
+    isls = [synth.noise_island((40, 36, 28), seed=91), synth.noise_island((30, 28, 20), seed=92)]
+
+    def pinned(a):
+        t = torch.empty(a.size, dtype={np.float32: torch.float32, np.uint8: torch.uint8}[a.dtype.type],
+                        pin_memory=True)
+        v = t.numpy()
+        v[:] = a.reshape(-1)
+        return t, v
+
+    keep, phis = [], []
+    for k, isl in enumerate(isls):
+        assert e.add_island(k + 1, isl.dims) == capi.PFSF_OK
+        if k == 0:
+            arrs = [np.zeros(isl.n, np.float32), isl.source.copy(), isl.kappa.copy(), isl.vtype.copy()]
+        else:
+            ts = [pinned(np.zeros(isl.n, np.float32)), pinned(isl.source), pinned(isl.kappa), pinned(isl.vtype)]
+            keep.append(ts)
+            arrs = [v for _, v in ts]
+        keep.append(arrs)
+        phis.append(arrs[0])
+        assert e.register_kappa(k + 1, *arrs) == capi.PFSF_OK
+    for rep in range(2):  # the second solve replays the captured launch
+        for p in phis:
+            p[:] = 0.0
+        rc, st = e.solve([1, 2], tol=1e-6, flags=capi.SOLVE_COLD_START)
+        assert rc == capi.PFSF_OK and st.islands_converged == 2 and st.max_rel_residual <= 1e-6
+        for k, isl in enumerate(isls):
+            rc, x64 = e.read_solution64(k + 1, isl.n)
+            assert rc == capi.PFSF_OK
+            assert np.array_equal(phis[k].view(np.uint32), x64.astype(np.float32).view(np.uint32)), (rep, k)
+            assert np.abs(phis[k]).max() > 0.0
+    e.close()
