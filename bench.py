@@ -789,6 +789,10 @@ def run_tick_dbb(args):
         "voxel_updates_per_s": 16.0 * meta["grid_total"] / (dev_ms * 1e-3),
         "gpu_launches": int(np.mean([r.kernel_launches for r in reps])),
         "groups": int(reps[-1].groups), "graph_replayed": int(reps[-1].graph_replayed),
+        "host_ms_per_tick": float(np.mean([r.host_us for r in reps])) * 1e-3,
+        "host_ms_by_graph_use": {k: (float(np.mean([r.host_us for r in reps if r.graph_replayed == v])) * 1e-3
+                                     if any(r.graph_replayed == v for r in reps) else None)
+                                 for k, v in (("replayed", 1), ("updated", 2), ("instantiated", 0))},
         "graph_use": {"replayed": sum(r.graph_replayed == 1 for r in reps),
                       "updated": sum(r.graph_replayed == 2 for r in reps),
                       "instantiated": sum(r.graph_replayed == 0 for r in reps)},

@@ -211,7 +211,8 @@ typedef struct pfsf_tick_report {
     double grid_voxels;        /* voxels of the dispatched islands' boxes */
     float device_ms;           /* engine-stream time from the table upload to the
                                   result copy (CUDA events) */
-    int32_t reserved;
+    int32_t host_us;           /* host time from the call's planning to the graph launch (planning,
+                                  table, and any capture, update or instantiation), microseconds */
 } pfsf_tick_report;
 
 PFSF_API pfsf_result pfsf_last_tick_report(pfsf_engine engine, pfsf_tick_report* out);

@@ -19,6 +19,7 @@
 // readback into its stress buffer are kernels over the device-visible
 // mappings of those arrays, inside the graph.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -124,6 +125,7 @@ void Engine::free_tick_batch() {
 pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_cap,
                                  const std::vector<const float*>* phi_in) {
     if (set.empty()) return PFSF_OK;
+    const auto host_t0 = std::chrono::steady_clock::now();
     if (!tbatch_) tbatch_.reset(new TickBatch());
     TickBatch& B = *tbatch_;
     const int nisl = (int)set.size();
@@ -516,6 +518,7 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
         B.key = key;
         B.graph_launches = nl;
     }
+    const auto host_t1 = std::chrono::steady_clock::now();
     if (!CU_OK(cudaGraphLaunch(B.exec, stream_))) return PFSF_ERROR_VULKAN;
     launches_ += B.graph_launches;
     // stress buffers that could not be mapped: copied
@@ -537,6 +540,8 @@ pfsf_result Engine::tick_batched(const std::vector<Island*>& set, int32_t want_c
     R.groups = tail_only ? 1 : ng;
     R.graph_replayed = replayed ? 1 : (updated ? 2 : 0);
     R.kernel_launches = B.graph_launches;
+    R.host_us = (int32_t)std::min<int64_t>(
+        INT32_MAX, std::chrono::duration_cast<std::chrono::microseconds>(host_t1 - host_t0).count());
     for (int j = 0; j < nisl; j++) {
         const Island& s = *set[order[j]];
         R.algorithmic_bytes += tick_bytes(s, plan[order[j]], tail_only, cfg_.enable_phase_field, want_cap > 0,

@@ -103,7 +103,7 @@ class IslandReport(C.Structure):
 class TickReport(C.Structure):
     _fields_ = [("struct_bytes", C.c_int32), ("islands", C.c_int32), ("groups", C.c_int32),
                 ("graph_replayed", C.c_int32), ("kernel_launches", C.c_int64), ("algorithmic_bytes", C.c_double),
-                ("grid_voxels", C.c_double), ("device_ms", C.c_float), ("reserved", C.c_int32)]
+                ("grid_voxels", C.c_double), ("device_ms", C.c_float), ("host_us", C.c_int32)]
 
 
 MG_V, MG_W = 0, 1
