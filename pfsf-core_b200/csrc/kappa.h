@@ -95,6 +95,11 @@ struct KArena {
     // update vectors, coarse update vector, per-step coefficients
     float* dinv0;
     float* d0;
+    // per fine voxel: 1/kappa of the preconditioner's kappa and of the FP32
+    // kappa (rcp.approx: +inf on air), written once per solve; the marching
+    // passes copy them into shared memory with cp.async
+    float* rkp;
+    float* rk32;
     float* cd;
     int smoother;          // 0 symmetric 8-colour Gauss-Seidel, 1 Chebyshev
     int wcycle;            // 1: W-cycle (levels below level 1 visited twice), 0: V-cycle

@@ -554,7 +554,8 @@ __device__ void team_solve(const KArena& A, KDesc& D, TeamT& tm) {
     if constexpr (TeamT::kFlat) {
         // the marching passes never write non-solid voxels: q starts at zero
         vop_zero(t, T, (int)D.n, A.q + D.off);
-        flat_lists(A, D, *tm.fs, tm);
+        op_rk<P>(A, D, t, T);
+        flat_lists(A, D, *tm.fs, tm);  // ends with a team barrier
     }
     if (tm.leader()) D.t_setup = globaltimer() - D.t_start;
     // time in V-cycles (the leader's clock, between barriers)

@@ -49,19 +49,20 @@ const void* map_arena_host(Island& s, void* p, int64_t bytes, std::vector<void*>
 double solve_bytes(const KDesc& d, int prec, int nu, int coarse_sweeps, int smoother, int cheb_k, int wcycle) {
     const double kb = prec > 0 ? 2.0 : 4.0;   // preconditioner kappa
     const double cb = prec > 0 ? 2.0 : 4.0;   // coarse coefficient
-    const double wf = kb;                     // fine-level weights come from kappa
+    const double wf = 4.0;                    // fine-level weights: the 1/kappa array of the solve
     const double n0 = (double)d.n;
     const double cell = 26.0 * cb + 4.0;      // coefficients + diagonal
-    double setup = 0.0, vc = 0.0;
+    double setup = n0 * (kb + 4.0 + 8.0);     // the two 1/kappa arrays (op_rk)
+    double vc = 0.0;
     if (d.nlev > 1) {
-        setup += n0 * (wf + 1.0) + (double)d.lev[1].n * cell;
+        setup += n0 * (kb + 1.0) + (double)d.lev[1].n * cell;
         for (int l = 1; l < d.nlev - 1; l++) setup += (double)d.lev[l].n * cell + (double)d.lev[l + 1].n * cell;
         if (smoother == 1) {
             // Chebyshev: first step (r, dinv -> d, z), then per step a stencil
             // pass (weights, type, z, r, dinv, d rw) and an update pass (d, z rw, type)
             const double step = (wf + 1.0 + 4.0 + 4.0 + 4.0 + 8.0) + (4.0 + 8.0 + 1.0);
             vc += n0 * 16.0 + (2.0 * cheb_k - 1.0) * n0 * step;
-            setup += n0 * (wf + 1.0 + 4.0);  // inverse diagonal
+            setup += n0 * (kb + 1.0 + 4.0);  // inverse diagonal
         } else {
             vc += 2.0 * nu * n0 * (wf + 1.0 + 8.0 + 4.0);      // fine GS sweeps: weights, type, z rw, r
         }
@@ -173,7 +174,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
                  o_cx = take(coarse * 4), o_cb = take(coarse * 4), o_desc = take(sizeof(KDesc) * nisl),
                  o_order = take(sizeof(int) * nisl), o_queue = take(256),
                  o_scr = take(sizeof(float) * kappa::plain_scratch_floats()), o_dinv = take(fine * 4),
-                 o_d0 = take(fine * 4), o_cdd = take(coarse * 4), o_cx2 = take(coarse * 4),
+                 o_d0 = take(fine * 4), o_rkp = take(fine * 4), o_rk32 = take(fine * 4), o_cdd = take(coarse * 4),
+                 o_cx2 = take(coarse * 4),
                  o_flist = take(fine * 4), o_fstart = take((size_t)std::max<int64_t>(starts, 1) * 4),
                  o_io = take(sizeof(kappa::IslandIO) * nisl);
     A->bytes = off;
@@ -211,6 +213,8 @@ bool Engine::build_arena(const std::vector<Island*>& set) {
     k.scratch = reinterpret_cast<float*>(b + o_scr);
     k.dinv0 = reinterpret_cast<float*>(b + o_dinv);
     k.d0 = reinterpret_cast<float*>(b + o_d0);
+    k.rkp = reinterpret_cast<float*>(b + o_rkp);
+    k.rk32 = reinterpret_cast<float*>(b + o_rk32);
     k.cd = reinterpret_cast<float*>(b + o_cdd);
     k.cx2 = reinterpret_cast<float*>(b + o_cx2);
     k.flist = reinterpret_cast<uint32_t*>(b + o_flist);
@@ -681,12 +685,11 @@ pfsf_result Engine::debug_time_pass(int32_t id, int32_t pass, int32_t reps, floa
     cudaEventDestroy(e1);
     launches_++;
     if (!ok) return PFSF_ERROR_VULKAN;
-    // algorithmic bytes: the march stages the input vector and kappa of every
-    // cell of the island's box; the solid voxels read and write the rest
+    // algorithmic bytes: the march stages the input vector and 1/kappa of
+    // every cell of the island's box; the solid voxels read and write the rest
     const double n = (double)arena_->desc[q].n, na = (double)arena_->active[q];
-    const double kb = k.prec > 0 ? 2.0 : 4.0;
-    const double per = pass == 0 ? (4.0 + kb) * n + (4.0 + 4.0 + 8.0 + 4.0 + 4.0) * na  // r, dinv, d rw, zout, list
-                                 : (4.0 + 4.0) * n + (4.0 + 4.0) * na;                     // p, k32; q, list
+    const double per = pass == 0 ? (4.0 + 4.0) * n + (4.0 + 4.0 + 8.0 + 4.0 + 4.0) * na  // r, dinv, d rw, zout, list
+                                 : (4.0 + 4.0) * n + (4.0 + 4.0) * na;                     // p, 1/k32; q, list
     *ms = t / (float)reps;
     *bytes = per;
     return PFSF_OK;

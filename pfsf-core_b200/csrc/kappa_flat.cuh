@@ -9,16 +9,16 @@
 // stencil arithmetic of their solid neighbours in the warp.  Here a CTA takes
 // a work item of tx x ty columns (kFlatCap cells per plane with the one-voxel
 // halo, see flat_tile) by a run of planes and marches up the planes with a
-// 4-plane ring of the input vector and of 1/kappa in shared memory: plane
-// z+2 is fetched into registers while plane z is computed, then stored into
-// the slot plane z-2 used.  Plane z is computed only at its solid voxels,
+// 5-plane ring of the input vector and of 1/kappa in shared memory: plane
+// z+3 is copied by cp.async (no registers) into the slot plane z-2 used
+// while plane z is computed.  Plane z is computed only at its solid voxels,
 // taken from a list per (tile, plane) built once per solve (flat_lists), so
 // every active lane does stencil work.
 //
 // Link weight.  The harmonic mean is evaluated as kappa_i kappa_j /
 // (kappa_i + kappa_j) = 1 / (1/kappa_i + 1/kappa_j), with the reciprocals
-// staged once per cell (rcp.approx: 1/0 = +inf, so an air or out-of-box
-// neighbour gets weight 1/(r_i + inf) = 0 with no test), and the 26 terms
+// written once per solve (op_rk; rcp.approx: 1/0 = +inf, so an air or
+// out-of-box neighbour gets weight 1/(r_i + inf) = 0 with no test), and the 26 terms
 // are summed per link class (faces x2, edges x1, corners x1/3).  Results
 // equal the generic ops' up to FP32 rounding; both are the same operator.
 //
@@ -33,9 +33,13 @@ namespace pfsf_b200 {
 namespace kappa {
 namespace {
 
+// Ring of kFlatRing planes: z-1, z, z+1 in use, z+2 landed or landing,
+// z+3 in flight (issued at step z).
+constexpr int kFlatRing = 5;
 struct FlatSmem {
-    float v[4][kFlatCap];  // vector ring
-    float w[4][kFlatCap];  // 1/kappa ring
+    float v[kFlatRing][kFlatCap];  // vector ring
+    float w[kFlatRing][kFlatCap];  // 1/kappa ring
+    float spare[kFlatCap];         // per-column scratch of the residual restriction
 };
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -43,7 +47,19 @@ __device__ __forceinline__ float rcp_approx(float x) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
-__device__ __forceinline__ int fslot(int z) { return (z + 4) & 3; }
+__device__ __forceinline__ int fslot(int z) { return (z + kFlatRing) % kFlatRing; }
+
+// 4-byte global -> shared copies that bypass registers (completion per
+// thread by commit groups; a CTA barrier after the wait publishes them)
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 struct FlatGeom {
     int tx, ty, hx, hp, ntx, ntiles, zc, nwork;
@@ -82,7 +98,7 @@ __device__ __forceinline__ FlatGeom flat_geom(const KDesc& D, int ncta) {
 
 struct FlatPlanes {
     const float *vm, *v0, *vp, *wm, *w0, *wp;
-    float* spare;  // the vector slot of plane z-2: free until the step ends
+    float* spare;  // per-column scratch (FlatSmem::spare)
 };
 
 // 26-neighbour sum of w_ij (z_i - z_j) at halo cell hc
@@ -120,30 +136,54 @@ __device__ __forceinline__ void flat_entries(const uint32_t* L, int b0, int b1,
 
 // March over every work item this CTA owns (cta, cta + ncta, ...).
 // body(tile, x0, y0, z, z0, z1, planes, entries) runs on every thread once
-// per plane (it may hold CTA barriers); vload / kload read the vector and
-// kappa of island voxel g.  With kList the march also pipelines the solid
-// lists (L, st): entries of plane z+1 and the list bounds of plane z+2 load
-// while plane z is computed, so a step waits on one round of global loads
-// (the per-voxel operands), not three.
-template <bool kList, class VLoad, class KLoad, class Body>
+// per plane (it may hold CTA barriers); vsrc and wsrc are the island's
+// vector and 1/kappa arrays.  The planes stream into a shared-memory ring by
+// cp.async three planes ahead of the one computed, so a plane step waits on
+// no global load of its own (out-of-box cells are stored directly: vector 0,
+// 1/kappa +inf, which gives their links weight 0).  With kList the march
+// also pipelines the solid lists (L, st): entries of plane z+1 and the list
+// bounds of plane z+2 load while plane z is computed.
+template <bool kList, class Body>
 __device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int cta, int ncta, const uint32_t* L,
-                           const int* st, VLoad vload, KLoad kload, Body body) {
+                           const int* st, const float* vsrc, const float* wsrc, Body body) {
     constexpr int J = kFlatCap / kFlatThreads;
     const int tid = threadIdx.x;
+    const int lxly = D.lx * D.ly;
     for (int w = cta; w < G.nwork; w += ncta) {
         const int tile = w % G.ntiles, zk = w / G.ntiles;
         const int x0 = (tile % G.ntx) * G.tx, y0 = (tile / G.ntx) * G.ty;
         const int z0 = zk * G.zc, z1 = min(z0 + G.zc, D.lz);
-        auto fetch = [&](int z, int e, float& v, float& k) {
-            v = 0.0f;
-            k = 0.0f;
-            if (e >= G.hp || z < 0 || z >= D.lz) return;
-            const int hy = e / G.hx, hx = e - hy * G.hx;
-            const int x = x0 - 1 + hx, y = y0 - 1 + hy;
-            if (x < 0 || x >= D.lx || y < 0 || y >= D.ly) return;
-            const int g = x + D.lx * (y + D.ly * z);
-            v = vload(g);
-            k = kload(g);
+        // this thread's cells of the halo plane: column index in the island,
+        // -1 outside the island's box, -2 past the plane
+        int col[J];
+#pragma unroll
+        for (int j = 0; j < J; j++) {
+            const int e = tid + kFlatThreads * j;
+            col[j] = -2;
+            if (e < G.hp) {
+                const int hy = e / G.hx, hx = e - hy * G.hx;
+                const int x = x0 - 1 + hx, y = y0 - 1 + hy;
+                col[j] = (x < 0 || x >= D.lx || y < 0 || y >= D.ly) ? -1 : x + D.lx * y;
+            }
+        }
+        auto issue = [&](int z) {
+            float* vs = S.v[fslot(z)];
+            float* ws = S.w[fslot(z)];
+            const bool inz = z >= 0 && z < D.lz;
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const int e = tid + kFlatThreads * j;
+                if (col[j] == -2) continue;
+                if (col[j] < 0 || !inz) {
+                    vs[e] = 0.0f;
+                    ws[e] = __int_as_float(0x7f800000);
+                } else {
+                    const int g = col[j] + lxly * z;
+                    cp_async4(vs + e, vsrc + g);
+                    cp_async4(ws + e, wsrc + g);
+                }
+            }
+            cp_async_commit();
         };
         uint32_t cur[J], nxt[J];
         int nb0 = 0, nb1 = 0;  // list bounds of plane z+1 (then z+2)
@@ -155,23 +195,11 @@ __device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int c
                 nb1 = st[p + 2];
             }
         }
-        for (int pz = z0 - 1; pz <= z0 + 1; pz++) {
-#pragma unroll
-            for (int j = 0; j < J; j++) {
-                const int e = tid + kFlatThreads * j;
-                float v, k;
-                fetch(pz, e, v, k);
-                if (e < G.hp) {
-                    S.v[fslot(pz)][e] = v;
-                    S.w[fslot(pz)][e] = rcp_approx(k);
-                }
-            }
-        }
+        for (int pz = z0 - 1; pz <= z0 + 2; pz++) issue(pz);
+        cp_async_wait<1>();  // planes z0-1 .. z0+1 landed
         __syncthreads();
         for (int z = z0; z < z1; z++) {
-            float pv[J], pk[J];
-#pragma unroll
-            for (int j = 0; j < J; j++) fetch(z + 2, tid + kFlatThreads * j, pv[j], pk[j]);
+            issue(z + 3);  // into the slot of plane z-2, last read in step z-1
             if constexpr (kList) {
                 flat_entries(L, nb0, nb1, nxt);
                 const int p2 = tile * D.lz + z + 2;
@@ -179,22 +207,31 @@ __device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int c
                 nb1 = z + 2 < z1 ? st[p2 + 1] : 0;
             }
             const FlatPlanes P{S.v[fslot(z - 1)], S.v[fslot(z)], S.v[fslot(z + 1)],
-                               S.w[fslot(z - 1)], S.w[fslot(z)], S.w[fslot(z + 1)], S.v[fslot(z + 2)]};
+                               S.w[fslot(z - 1)], S.w[fslot(z)], S.w[fslot(z + 1)], S.spare};
             body(tile, x0, y0, z, z0, z1, P, cur);
-#pragma unroll
-            for (int j = 0; j < J; j++) {
-                const int e = tid + kFlatThreads * j;
-                if (e < G.hp) {
-                    S.v[fslot(z + 2)][e] = pv[j];
-                    S.w[fslot(z + 2)][e] = rcp_approx(pk[j]);
-                }
-            }
             if constexpr (kList) {
 #pragma unroll
                 for (int j = 0; j < J; j++) cur[j] = nxt[j];
             }
+            cp_async_wait<1>();  // plane z+2 landed (z+3 may still be in flight)
             __syncthreads();
         }
+        cp_async_wait<0>();  // nothing in flight into the ring past this work item
+        __syncthreads();
+    }
+}
+
+// 1/kappa of every voxel of the island, for the marching passes (the values
+// they staged per plane before: rcp.approx of the preconditioner's kappa and
+// of the FP32 kappa, +inf on air)
+template <int P>
+__device__ void op_rk(const KArena& A, const KDesc& D, int t, int T) {
+    const Fine F = fine_view(A, D);
+    float* rkp = A.rkp + D.off;
+    float* rk32 = A.rk32 + D.off;
+    for (int i = t; i < F.n; i += T) {
+        rkp[i] = rcp_approx(kpre<P>(F, i));
+        rk32[i] = rcp_approx(F.k32[i]);
     }
 }
 
@@ -293,7 +330,7 @@ __device__ void fop_cheb0_dz(const KArena& A, const KDesc& D, FlatSmem& S, int c
     const uint32_t* L = A.flist + D.off;
     const int* st = A.fstart + D.soff;
     const FlatGeom G = flat_geom(D, ncta);
-    flat_march<true>(D, G, S, cta, ncta, L, st, [&](int g) { return zin[g]; }, [&](int g) { return kpre<P>(F, g); },
+    flat_march<true>(D, G, S, cta, ncta, L, st, zin, A.rkp + D.off,
                      [&](int, int x0, int y0, int z, int, int, const FlatPlanes& Pl, const uint32_t(&ent)[kFlatCap / kFlatThreads]) {
 #pragma unroll
                          for (int k = 0; k < kFlatCap / kFlatThreads; k++) {
@@ -319,7 +356,7 @@ __device__ void fop_matvec(const KArena& A, const KDesc& D, FlatSmem& S, int cta
     const uint32_t* L = A.flist + D.off;
     const int* st = A.fstart + D.soff;
     const FlatGeom G = flat_geom(D, ncta);
-    flat_march<true>(D, G, S, cta, ncta, L, st, [&](int g) { return F.p[g]; }, [&](int g) { return F.k32[g]; },
+    flat_march<true>(D, G, S, cta, ncta, L, st, F.p, A.rk32 + D.off,
                      [&](int, int x0, int y0, int z, int, int, const FlatPlanes& Pl, const uint32_t(&ent)[kFlatCap / kFlatThreads]) {
 #pragma unroll
                          for (int k = 0; k < kFlatCap / kFlatThreads; k++) {
@@ -339,7 +376,7 @@ __device__ void fop_matvec(const KArena& A, const KDesc& D, FlatSmem& S, int cta
 // Residual of level 0 (operator A') summed over each 2x2x2 aggregate into
 // level 1, x1 = 0.  Every column of the tile, solid or not, keeps one thread
 // for the whole march: plane pairs add in registers, then the 2 x 2 column
-// groups through the ring's spare slot.  Tiles and work items start on even x, y, z,
+// groups through the spare scratch.  Tiles and work items start on even x, y, z,
 // so every aggregate lies in one work item.  (Summation order differs from
 // op_restrict0's child order: equal up to FP32 rounding.)
 template <int P>
@@ -358,8 +395,7 @@ __device__ void fop_restrict0(const KArena& A, const KDesc& D, FlatSmem& S, int 
         cxj[j] = c - cyj[j] * G.tx;
     }
     float hold[J];
-    flat_march<false>(D, G, S, cta, ncta, nullptr, nullptr, [&](int g) { return F.z[g]; },
-                      [&](int g) { return kpre<P>(F, g); },
+    flat_march<false>(D, G, S, cta, ncta, nullptr, nullptr, F.z, A.rkp + D.off,
                       [&](int, int x0, int y0, int z, int z0, int z1, const FlatPlanes& Pl,
                           const uint32_t(&)[kFlatCap / kFlatThreads]) {
                    const bool second = ((z - z0) & 1) != 0;
@@ -403,7 +439,7 @@ __device__ void fop_restrict0(const KArena& A, const KDesc& D, FlatSmem& S, int 
                            C.x[c] = 0.0f;
                        }
                    }
-                   __syncthreads();  // the march stores plane z+2 into the spare slot next
+                   __syncthreads();  // the spare is written again at the next plane pair
                });
 }
 
