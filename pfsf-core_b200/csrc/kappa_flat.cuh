@@ -9,8 +9,8 @@
 // stencil arithmetic of their solid neighbours in the warp.  Here a CTA takes
 // a work item of tx x ty columns (kFlatCap cells per plane with the one-voxel
 // halo, see flat_tile) by a run of planes and marches up the planes with a
-// 5-plane ring of the input vector and of 1/kappa in shared memory: plane
-// z+3 is copied by cp.async (no registers) into the slot plane z-2 used
+// 4-plane ring of the input vector and of 1/kappa in shared memory: plane
+// z+2 is copied by cp.async (no registers) into the slot plane z-2 used
 // while plane z is computed.  Plane z is computed only at its solid voxels,
 // taken from a list per (tile, plane) built once per solve (flat_lists), so
 // every active lane does stencil work.
@@ -34,8 +34,16 @@ namespace kappa {
 namespace {
 
 // Ring of kFlatRing planes: z-1, z, z+1 in use, z+2 landed or landing,
-// z+3 in flight (issued at step z).
-constexpr int kFlatRing = 5;
+// planes up to z + kFlatAhead in flight (plane z + kFlatAhead issued at step
+// z).  Measured on the 4096-island solve: 4 slots 333 ms, 5 slots 344 ms,
+// 6 slots 368 ms -- the shared memory of two CTAs per SM comes out of the
+// L1 that the rest of the solve relies on.
+#ifndef PFSF_FLAT_RING
+#define PFSF_FLAT_RING 4
+#endif
+constexpr int kFlatRing = PFSF_FLAT_RING;
+constexpr int kFlatAhead = kFlatRing - 2;
+static_assert(kFlatRing >= 4, "three planes in use and one landing");
 struct FlatSmem {
     float v[kFlatRing][kFlatCap];  // vector ring
     float w[kFlatRing][kFlatCap];  // 1/kappa ring
@@ -195,11 +203,11 @@ __device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int c
                 nb1 = st[p + 2];
             }
         }
-        for (int pz = z0 - 1; pz <= z0 + 2; pz++) issue(pz);
-        cp_async_wait<1>();  // planes z0-1 .. z0+1 landed
+        for (int pz = z0 - 1; pz < z0 + kFlatAhead; pz++) issue(pz);
+        cp_async_wait<kFlatAhead - 2>();  // planes z0-1 .. z0+1 landed
         __syncthreads();
         for (int z = z0; z < z1; z++) {
-            issue(z + 3);  // into the slot of plane z-2, last read in step z-1
+            issue(z + kFlatAhead);  // into the slot of plane z-2, last read in step z-1
             if constexpr (kList) {
                 flat_entries(L, nb0, nb1, nxt);
                 const int p2 = tile * D.lz + z + 2;
@@ -213,7 +221,7 @@ __device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int c
 #pragma unroll
                 for (int j = 0; j < J; j++) cur[j] = nxt[j];
             }
-            cp_async_wait<1>();  // plane z+2 landed (z+3 may still be in flight)
+            cp_async_wait<kFlatAhead - 2>();  // plane z+2 landed (later ones may still be in flight)
             __syncthreads();
         }
         cp_async_wait<0>();  // nothing in flight into the ring past this work item
