@@ -47,7 +47,6 @@ static_assert(kFlatRing >= 4, "three planes in use and one landing");
 struct FlatSmem {
     float v[kFlatRing][kFlatCap];  // vector ring
     float w[kFlatRing][kFlatCap];  // 1/kappa ring
-    float spare[kFlatCap];         // per-column scratch of the residual restriction
 };
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -106,7 +105,7 @@ __device__ __forceinline__ FlatGeom flat_geom(const KDesc& D, int ncta) {
 
 struct FlatPlanes {
     const float *vm, *v0, *vp, *wm, *w0, *wp;
-    float* spare;  // per-column scratch (FlatSmem::spare)
+    float* spare;  // the vector slot of plane z-1: free once this step's stencils have read it
 };
 
 // 26-neighbour sum of w_ij (z_i - z_j) at halo cell hc
@@ -215,7 +214,7 @@ __device__ void flat_march(const KDesc& D, const FlatGeom& G, FlatSmem& S, int c
                 nb1 = z + 2 < z1 ? st[p2 + 1] : 0;
             }
             const FlatPlanes P{S.v[fslot(z - 1)], S.v[fslot(z)], S.v[fslot(z + 1)],
-                               S.w[fslot(z - 1)], S.w[fslot(z)], S.w[fslot(z + 1)], S.spare};
+                               S.w[fslot(z - 1)], S.w[fslot(z)], S.w[fslot(z + 1)], S.v[fslot(z - 1)]};
             body(tile, x0, y0, z, z0, z1, P, cur);
             if constexpr (kList) {
 #pragma unroll
@@ -384,7 +383,8 @@ __device__ void fop_matvec(const KArena& A, const KDesc& D, FlatSmem& S, int cta
 // Residual of level 0 (operator A') summed over each 2x2x2 aggregate into
 // level 1, x1 = 0.  Every column of the tile, solid or not, keeps one thread
 // for the whole march: plane pairs add in registers, then the 2 x 2 column
-// groups through the spare scratch.  Tiles and work items start on even x, y, z,
+// groups through the vector slot of plane z-1 (no longer needed once the
+// plane's stencils are done).  Tiles and work items start on even x, y, z,
 // so every aggregate lies in one work item.  (Summation order differs from
 // op_restrict0's child order: equal up to FP32 rounding.)
 template <int P>
@@ -423,6 +423,7 @@ __device__ void fop_restrict0(const KArena& A, const KDesc& D, FlatSmem& S, int 
                        hold[j] = second ? hold[j] + res : res;
                    }
                    if (!second && z != z1 - 1) return;
+                   __syncthreads();  // every stencil of this plane has read plane z-1
 #pragma unroll
                    for (int j = 0; j < J; j++) {
                        const int c = tid + kFlatThreads * j;
@@ -447,7 +448,7 @@ __device__ void fop_restrict0(const KArena& A, const KDesc& D, FlatSmem& S, int 
                            C.x[c] = 0.0f;
                        }
                    }
-                   __syncthreads();  // the spare is written again at the next plane pair
+                   __syncthreads();  // the slot is refilled by the next step's copies
                });
 }
 
